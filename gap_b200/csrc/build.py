@@ -1,0 +1,82 @@
+"""Build the native libraries in-tree (gap_b200/lib/).
+
+    python -m gap_b200.csrc.build          # or gap_b200.csrc.build.build()
+
+Everything is compiled for sm_100a only (-gencode arch=compute_100a,code=sm_100a).  nvcc
+cross-compiles without a GPU.  Rebuilds a target only when one of its sources is newer.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+ROOT = os.path.dirname(PKG)
+LIB = os.path.join(PKG, "lib")
+INCLUDE = os.path.join(ROOT, "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++20", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+              "--expt-relaxed-constexpr", "-I" + INCLUDE] + ARCH
+
+
+def _nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    return r
+
+
+CORE_SOURCES = ["symbolic.cpp", "nr.cu", "ybus.cu"]
+HEADERS = ["internal.h", "blocks.cuh", "nr_kernels.cuh"]
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile libgapk.so; returns its path."""
+    os.makedirs(LIB, exist_ok=True)
+    nvcc = _nvcc()
+    objdir = os.path.join(LIB, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    hdrs = [os.path.join(HERE, h) for h in HEADERS] + [os.path.join(INCLUDE, "gapk.h")]
+    objs = []
+    for src in CORE_SOURCES:
+        s = os.path.join(HERE, src)
+        o = os.path.join(objdir, src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs):
+            cmd = [nvcc] + NVCC_FLAGS + ["-c", s, "-o", o]
+            if src.endswith(".cpp"):
+                cmd = [nvcc] + NVCC_FLAGS + ["-x", "c++", "-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+    so = os.path.join(LIB, "libgapk.so")
+    if force or _stale(so, objs):
+        cmd = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", so] + objs
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    return so
+
+
+if __name__ == "__main__":
+    p = build(verbose="-v" in sys.argv, force="-f" in sys.argv)
+    print(p)

@@ -1,0 +1,667 @@
+// Host side of the Newton-Raphson engine: plan upload, batch state, the device-resident
+// iteration loop (CUDA graph with a conditional while node), and the gapk_nr_* C ABI.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gapk.h"
+#include "internal.h"
+#include "nr_kernels.cuh"
+
+namespace gapk {
+
+namespace {
+thread_local std::string g_err = "no error";
+}
+void set_error(std::string const& msg) { g_err = msg; }
+
+#define GAPK_CUDA_TRY(expr)                                                         \
+    do {                                                                            \
+        cudaError_t e__ = (expr);                                                   \
+        if (e__ != cudaSuccess) {                                                   \
+            set_error(std::string(#expr) + ": " + cudaGetErrorString(e__));         \
+            return e__ == cudaErrorMemoryAllocation ? GAPK_ENOMEM : GAPK_ECUDA;     \
+        }                                                                           \
+    } while (0)
+
+// ---- device buffers -------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(DevBuf const&) = delete;
+    DevBuf& operator=(DevBuf const&) = delete;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    int alloc(size_t n) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = n;
+        if (n == 0) return GAPK_OK;
+        GAPK_CUDA_TRY(cudaMalloc(&p, n));
+        return GAPK_OK;
+    }
+    template <typename V>
+    int upload(std::vector<V> const& v) {
+        int rc = alloc(v.size() * sizeof(V));
+        if (rc) return rc;
+        if (!v.empty()) GAPK_CUDA_TRY(cudaMemcpy(p, v.data(), bytes, cudaMemcpyHostToDevice));
+        return GAPK_OK;
+    }
+    template <typename P>
+    P* as() const {
+        return reinterpret_cast<P*>(p);
+    }
+};
+
+}  // namespace gapk
+
+using namespace gapk;
+
+struct gapk_nr_plan_s {
+    NRPlanHost h;
+    std::vector<int> y_row_ptr, y_col;
+    // device copy (current device at first upload)
+    bool uploaded = false;
+    int device = -1;
+    DevBuf d_yrp, d_ycol, d_bt, d_nob, d_si, d_ss, d_sa, d_lp, d_ln, d_fa, d_tg, d_pr, d_fb,
+        d_sc, d_lptr, d_lidx, d_rptr, d_rl, d_arp, d_ar, d_var, d_eq;
+    PlanDev dev{};
+
+    int upload() {
+        if (uploaded) return GAPK_OK;
+        int rc = 0;
+        auto up = [&](DevBuf& b, std::vector<int> const& v) {
+            if (!rc) rc = b.upload(v);
+        };
+        up(d_yrp, y_row_ptr);
+        up(d_ycol, y_col);
+        up(d_bt, h.bus_type);
+        up(d_nob, h.node_of_bus);
+        up(d_si, h.slot_info);
+        up(d_ss, h.slot_src);
+        up(d_sa, h.slot_a);
+        up(d_lp, h.level_ptr);
+        up(d_ln, h.level_nodes);
+        up(d_fa, h.fa_ptr);
+        up(d_tg, h.targets);
+        up(d_pr, h.pairs);
+        up(d_fb, h.fb_ptr);
+        up(d_sc, h.scale);
+        up(d_lptr, h.lptr);
+        up(d_lidx, h.lidx);
+        up(d_rptr, h.rptr);
+        up(d_rl, h.rlist);
+        up(d_arp, h.arow_ptr);
+        up(d_ar, h.arow);
+        up(d_var, h.var_of_comp);
+        up(d_eq, h.eq_of_comp);
+        if (rc) return rc;
+        cudaGetDevice(&device);
+        dev.n_bus = h.n_bus;
+        dev.nb = h.nb;
+        dev.nnz_y = h.nnz_y;
+        dev.n_slots = h.n_slots;
+        dev.nnz_l = h.nnz_l;
+        dev.n_levels = h.n_levels;
+        dev.n_a = h.n_a;
+        dev.jac_mode = h.jac_mode;
+        dev.y_row_ptr = d_yrp.as<int>();
+        dev.y_col = d_ycol.as<int>();
+        dev.bus_type = d_bt.as<int>();
+        dev.node_of_bus = d_nob.as<int>();
+        dev.slot_info = d_si.as<int4>();
+        dev.slot_src = d_ss.as<int>();
+        dev.slot_a = d_sa.as<int>();
+        dev.level_ptr = d_lp.as<int>();
+        dev.level_nodes = d_ln.as<int>();
+        dev.fa_ptr = d_fa.as<int>();
+        dev.targets = d_tg.as<int4>();
+        dev.pairs = d_pr.as<int2>();
+        dev.fb_ptr = d_fb.as<int>();
+        dev.scale = d_sc.as<int2>();
+        dev.lptr = d_lptr.as<int>();
+        dev.lidx = d_lidx.as<int>();
+        dev.rptr = d_rptr.as<int>();
+        dev.rlist = d_rl.as<int2>();
+        dev.arow_ptr = d_arp.as<int>();
+        dev.arow = d_ar.as<int2>();
+        uploaded = true;
+        return GAPK_OK;
+    }
+};
+
+struct gapk_nr_batch_s {
+    gapk_nr_plan plan = nullptr;
+    int n_scen = 0, sw = 8, G = 0, precision = 0, y_shared = 1, threads = 256, use_graph = 1;
+    DevBuf V, Sspec, Scalc, Y, F, A64, rhs, dx, res, X, mis, state, solving, singular, iters,
+        status, fmis, gsolve, giter, ctrl, tol;
+    BatchDev dev{};
+    // graph cache
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_refine = -1;
+    int cur_refine = 0;
+    ~gapk_nr_batch_s() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace {
+
+inline unsigned blocks_for(long items, int threads) {
+    return static_cast<unsigned>((items + threads - 1) / threads);
+}
+
+template <typename T, int SW>
+void launch_body(gapk_nr_batch b, cudaStream_t st, int use_cond, cudaGraphConditionalHandle h) {
+    PlanDev const& P = b->plan->dev;
+    BatchDev const& B = b->dev;
+    const int G = b->G;
+    dim3 gm(blocks_for((long)P.n_bus * SW, 256), G);
+    k_mismatch<SW><<<gm, 256, 0, st>>>(P, B);
+    k_check<SW><<<1, 1024, 0, st>>>(B, use_cond, h);
+    dim3 gj(blocks_for((long)P.n_slots * SW, 256), G);
+    k_jfill<T, SW><<<gj, 256, 0, st>>>(P, B);
+    k_factor<T, SW><<<G, b->threads, 0, st>>>(P, B);
+    k_solve<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs, B.dx, 0);
+    for (int r = 0; r < b->cur_refine; ++r) {
+        dim3 gr(blocks_for((long)P.nb * SW, 256), G);
+        k_residual<SW><<<gr, 256, 0, st>>>(P, B);
+        k_solve<T, SW><<<G, b->threads, 0, st>>>(P, B, B.res, B.dx, 1);
+    }
+    dim3 gu(blocks_for((long)P.n_bus * SW, 256), G);
+    k_update<SW><<<gu, 256, 0, st>>>(P, B);
+}
+
+template <int SW>
+void launch_load(gapk_nr_batch b, const gapk_nr_inputs* in, cudaStream_t st) {
+    PlanDev const& P = b->plan->dev;
+    dim3 g(blocks_for((long)P.n_bus * SW, 256), b->G);
+    k_load<SW><<<g, 256, 0, st>>>(P, b->dev, reinterpret_cast<const double2*>(in->d_y),
+                                  reinterpret_cast<const double2*>(in->d_s_spec),
+                                  reinterpret_cast<const double2*>(in->d_v_init), in->d_u_pu);
+}
+
+template <int SW>
+void launch_store(gapk_nr_batch b, const gapk_nr_outputs* out, cudaStream_t st) {
+    PlanDev const& P = b->plan->dev;
+    long total = (long)b->n_scen * P.n_bus;
+    k_store<SW><<<blocks_for(total, 256), 256, 0, st>>>(
+        P, b->dev, reinterpret_cast<double2*>(out->d_v), out->d_iterations, out->d_status,
+        out->d_final_mismatch);
+}
+
+// dispatch on (precision, lanes)
+template <template <typename, int> class F, typename... A>
+int dispatch_tsw(int precision, int sw, A&&... a) {
+#define GAPK_CASE(T, S) F<T, S>::run(std::forward<A>(a)...)
+    if (precision == GAPK_PREC_FP64) {
+        switch (sw) {
+            case 1: GAPK_CASE(double, 1); return 0;
+            case 2: GAPK_CASE(double, 2); return 0;
+            case 4: GAPK_CASE(double, 4); return 0;
+            case 8: GAPK_CASE(double, 8); return 0;
+        }
+    } else {
+        switch (sw) {
+            case 1: GAPK_CASE(float, 1); return 0;
+            case 2: GAPK_CASE(float, 2); return 0;
+            case 4: GAPK_CASE(float, 4); return 0;
+            case 8: GAPK_CASE(float, 8); return 0;
+        }
+    }
+#undef GAPK_CASE
+    return -1;
+}
+
+template <typename T, int SW>
+struct BodyOp {
+    static void run(gapk_nr_batch b, cudaStream_t st, int uc, cudaGraphConditionalHandle h) {
+        launch_body<T, SW>(b, st, uc, h);
+    }
+};
+template <typename T, int SW>
+struct LoadOp {
+    static void run(gapk_nr_batch b, const gapk_nr_inputs* in, cudaStream_t st) {
+        launch_load<SW>(b, in, st);
+    }
+};
+template <typename T, int SW>
+struct StoreOp {
+    static void run(gapk_nr_batch b, const gapk_nr_outputs* out, cudaStream_t st) {
+        launch_store<SW>(b, out, st);
+    }
+};
+template <typename T, int SW>
+struct StageOp {
+    static void run(gapk_nr_batch b, int which, cudaStream_t st) {
+        PlanDev const& P = b->plan->dev;
+        BatchDev const& B = b->dev;
+        const int G = b->G;
+        switch (which) {
+            case 0: {
+                dim3 gm(blocks_for((long)P.n_bus * SW, 256), G);
+                k_mismatch<SW><<<gm, 256, 0, st>>>(P, B);
+                break;
+            }
+            case 1: {
+                dim3 gj(blocks_for((long)P.n_slots * SW, 256), G);
+                k_jfill<T, SW><<<gj, 256, 0, st>>>(P, B);
+                break;
+            }
+            case 2:
+                k_factor<T, SW><<<G, b->threads, 0, st>>>(P, B);
+                break;
+            case 3:
+                k_solve<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs, B.dx, 0);
+                for (int r = 0; r < b->cur_refine; ++r) {
+                    dim3 gr(blocks_for((long)P.nb * SW, 256), G);
+                    k_residual<SW><<<gr, 256, 0, st>>>(P, B);
+                    k_solve<T, SW><<<G, b->threads, 0, st>>>(P, B, B.res, B.dx, 1);
+                }
+                break;
+            case 4: {
+                dim3 gu(blocks_for((long)P.n_bus * SW, 256), G);
+                k_update<SW><<<gu, 256, 0, st>>>(P, B);
+                break;
+            }
+        }
+    }
+};
+template <typename T, int SW>
+struct ToRefOp {
+    static void run(gapk_nr_batch b, const double2* src, const int* map, int n_out, double sign,
+                    double* dst, cudaStream_t st) {
+        PlanDev const& P = b->plan->dev;
+        long total = (long)b->n_scen * P.nb;
+        if (total == 0) return;
+        k_node_to_ref<SW><<<blocks_for(total, 256), 256, 0, st>>>(src, P.nb, b->n_scen, n_out,
+                                                                   map, sign, dst);
+    }
+};
+
+int check_launch() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+        return GAPK_ECUDA;
+    }
+    return GAPK_OK;
+}
+
+int build_graph(gapk_nr_batch b, cudaStream_t st) {
+    if (b->exec && b->graph_refine == b->cur_refine) return GAPK_OK;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    GAPK_CUDA_TRY(cudaGraphCreate(&b->graph, 0));
+    cudaGraphConditionalHandle h;
+    GAPK_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, b->graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    GAPK_CUDA_TRY(cudaGraphAddNode(&node, b->graph, nullptr, 0, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    // capture the iteration body into the while node's graph
+    cudaStream_t cs;
+    GAPK_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        set_error(std::string("cudaStreamBeginCaptureToGraph: ") + cudaGetErrorString(e));
+        return GAPK_ECUDA;
+    }
+    dispatch_tsw<BodyOp>(b->precision, b->sw, b, cs, 1, h);
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(cs, &captured);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+        return GAPK_ECUDA;
+    }
+    GAPK_CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    b->graph_refine = b->cur_refine;
+    (void)st;
+    return GAPK_OK;
+}
+
+int load_inputs(gapk_nr_batch b, const gapk_nr_inputs* in, cudaStream_t st) {
+    if (!in || !in->d_y || !in->d_s_spec) {
+        set_error("inputs: d_y and d_s_spec are required");
+        return GAPK_EINVAL;
+    }
+    if (in->max_iterations < 0 || in->refine < 0 || in->refine > 8 ||
+        (in->policy != GAPK_POLICY_REFERENCE && in->policy != GAPK_POLICY_NEWTON)) {
+        set_error("inputs: bad max_iterations / refine / policy");
+        return GAPK_EINVAL;
+    }
+    if (in->refine > 0 && !b->A64.p) {
+        set_error("inputs: refine > 0 needs a batch created with precision FP32");
+        return GAPK_EINVAL;
+    }
+    b->cur_refine = in->refine;
+    int ctrl[5] = {0, in->max_iterations, 1, in->policy, 0};
+    GAPK_CUDA_TRY(cudaMemcpyAsync(b->ctrl.p, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, st));
+    double tol = in->tolerance;
+    GAPK_CUDA_TRY(cudaMemcpyAsync(b->tol.p, &tol, sizeof(double), cudaMemcpyHostToDevice, st));
+    dispatch_tsw<LoadOp>(b->precision, b->sw, b, in, st);
+    return check_launch();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gapk_last_error(void) { return g_err.c_str(); }
+int gapk_version(void) { return 100; }
+int gapk_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int gapk_nr_plan_create(int n_bus, int nnz_y, const int* h_y_row_ptr, const int* h_y_col_idx,
+                        const int* h_bus_type, const gapk_nr_plan_options* opt,
+                        gapk_nr_plan* out) {
+    if (!out || n_bus < 0 || nnz_y < 0 || !h_y_row_ptr || (nnz_y && !h_y_col_idx) ||
+        (n_bus && !h_bus_type)) {
+        set_error("gapk_nr_plan_create: bad arguments");
+        return GAPK_EINVAL;
+    }
+    int jac = opt ? opt->jacobian_mode : GAPK_JAC_REFERENCE;
+    int ord = opt ? opt->ordering : GAPK_ORDER_MINDEG;
+    if ((jac != 0 && jac != 1) || (ord != 0 && ord != 1)) {
+        set_error("gapk_nr_plan_create: bad options");
+        return GAPK_EINVAL;
+    }
+    auto p = std::make_unique<gapk_nr_plan_s>();
+    try {
+        if (!analyze_nr(n_bus, nnz_y, h_y_row_ptr, h_y_col_idx, h_bus_type, jac, ord, p->h))
+            return GAPK_EINVAL;
+    } catch (std::bad_alloc const&) {
+        set_error("gapk_nr_plan_create: host allocation failed");
+        return GAPK_ENOMEM;
+    }
+    p->y_row_ptr.assign(h_y_row_ptr, h_y_row_ptr + n_bus + 1);
+    p->y_col.assign(h_y_col_idx, h_y_col_idx + nnz_y);
+    *out = p.release();
+    return GAPK_OK;
+}
+
+int gapk_nr_plan_destroy(gapk_nr_plan p) {
+    delete p;
+    return GAPK_OK;
+}
+
+int gapk_nr_plan_get_info(gapk_nr_plan p, gapk_nr_plan_info* info) {
+    if (!p || !info) {
+        set_error("gapk_nr_plan_get_info: null argument");
+        return GAPK_EINVAL;
+    }
+    auto const& h = p->h;
+    info->n_bus = h.n_bus;
+    info->n_block = h.nb;
+    info->n_pq = h.n_pq;
+    info->n_pv = h.n_pv;
+    info->n_slack = h.n_slack;
+    info->n_vars = h.n_vars;
+    info->nnz_y = h.nnz_y;
+    info->nnz_l_blocks = h.nnz_l;
+    info->n_slots = h.n_slots;
+    info->n_a_blocks = h.n_a;
+    info->n_levels = h.n_levels;
+    info->n_pairs = h.n_pairs;
+    info->n_rows_pairs = h.nnz_l;
+    info->max_level_width = h.max_level_width;
+    return GAPK_OK;
+}
+
+int64_t gapk_nr_plan_export(gapk_nr_plan p, int what, int* h_buf) {
+    if (!p) return GAPK_EINVAL;
+    auto const& h = p->h;
+    std::vector<int> const* v = nullptr;
+    switch (what) {
+        case 0: v = &h.bus_of_node; break;
+        case 1: v = &h.node_pq; break;
+        case 2: v = &h.lptr; break;
+        case 3: v = &h.lidx; break;
+        case 4: v = &h.level_ptr; break;
+        case 5: v = &h.level_nodes; break;
+        case 6: v = &h.slot_info; break;
+        case 7: {
+            // slot_src_ptr derived from slot_info
+            int64_t n = h.n_slots + 1;
+            if (h_buf) {
+                for (int s = 0; s < h.n_slots; ++s) h_buf[s] = h.slot_info[4 * s + 2];
+                h_buf[h.n_slots] = static_cast<int>(h.slot_src.size());
+            }
+            return n;
+        }
+        case 8: v = &h.slot_src; break;
+        case 9: v = &h.fa_ptr; break;
+        case 10: v = &h.targets; break;
+        case 11: v = &h.pairs; break;
+        case 12: v = &h.fb_ptr; break;
+        case 13: v = &h.scale; break;
+        case 14: v = &h.rptr; break;
+        case 15: v = &h.rlist; break;
+        case 16: v = &h.var_of_comp; break;
+        case 17: v = &h.eq_of_comp; break;
+        case 18: v = &h.slot_a; break;
+        case 19: v = &h.arow_ptr; break;
+        case 20: v = &h.arow; break;
+        default:
+            set_error("gapk_nr_plan_export: unknown selector");
+            return GAPK_EINVAL;
+    }
+    if (h_buf && !v->empty()) std::memcpy(h_buf, v->data(), v->size() * sizeof(int));
+    return static_cast<int64_t>(v->size());
+}
+
+int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options* opt,
+                         gapk_nr_batch* out) {
+    if (!p || !out || n_scen <= 0) {
+        set_error("gapk_nr_batch_create: bad arguments");
+        return GAPK_EINVAL;
+    }
+    auto b = std::make_unique<gapk_nr_batch_s>();
+    b->plan = p;
+    b->n_scen = n_scen;
+    b->precision = opt ? opt->precision : GAPK_PREC_FP64;
+    b->y_shared = opt ? (opt->y_shared ? 1 : 0) : 1;
+    int lanes = opt ? opt->lanes : 0;
+    if (lanes == 0) lanes = n_scen >= 8 ? 8 : (n_scen >= 4 ? 4 : (n_scen >= 2 ? 2 : 1));
+    if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8) {
+        set_error("gapk_nr_batch_create: lanes must be 1, 2, 4 or 8");
+        return GAPK_EINVAL;
+    }
+    if (b->precision != GAPK_PREC_FP64 && b->precision != GAPK_PREC_FP32) {
+        set_error("gapk_nr_batch_create: bad precision");
+        return GAPK_EINVAL;
+    }
+    b->sw = lanes;
+    int thr = opt ? opt->threads : 0;
+    if (thr == 0) thr = lanes == 1 ? 512 : 256;
+    if (thr < 32 || thr > 1024 || thr % 32) {
+        set_error("gapk_nr_batch_create: threads must be a multiple of 32 in [32, 1024]");
+        return GAPK_EINVAL;
+    }
+    b->threads = thr;
+    b->use_graph = opt ? opt->use_graph : 1;
+    int rc = p->upload();
+    if (rc) return rc;
+    auto const& h = p->h;
+    const size_t G = (n_scen + lanes - 1) / lanes;
+    b->G = static_cast<int>(G);
+    const size_t L = G * lanes;
+    const size_t esz = b->precision == GAPK_PREC_FP64 ? 8 : 4;
+    const size_t n = h.n_bus, nb = h.nb;
+    auto A = [&](DevBuf& d, size_t bytes) {
+        if (!rc) rc = d.alloc(bytes < 16 ? 16 : bytes);
+    };
+    A(b->V, L * n * 16);
+    A(b->Sspec, L * n * 16);
+    A(b->Scalc, L * n * 16);
+    A(b->Y, (b->y_shared ? (size_t)h.nnz_y : L * h.nnz_y) * 16);
+    A(b->F, L * (size_t)h.n_slots * 4 * esz);
+    if (b->precision == GAPK_PREC_FP32) A(b->A64, L * (size_t)h.n_a * 32);
+    A(b->rhs, L * nb * 16);
+    A(b->dx, L * nb * 16);
+    A(b->res, L * nb * 16);
+    A(b->X, L * nb * 2 * esz);
+    A(b->mis, L * 8);
+    A(b->state, L * 4);
+    A(b->solving, L * 4);
+    A(b->singular, L * 4);
+    A(b->iters, L * 4);
+    A(b->status, L * 4);
+    A(b->fmis, L * 8);
+    A(b->gsolve, G * 4);
+    A(b->giter, G * 4);
+    A(b->ctrl, 8 * 4);
+    A(b->tol, 8);
+    if (rc) return rc;
+    BatchDev& d = b->dev;
+    d.n_scen = n_scen;
+    d.n_groups = b->G;
+    d.sw = lanes;
+    d.y_shared = b->y_shared;
+    d.V = b->V.as<double2>();
+    d.Sspec = b->Sspec.as<double2>();
+    d.Scalc = b->Scalc.as<double2>();
+    d.Y = b->Y.as<double2>();
+    d.F = b->F.p;
+    d.A64 = b->A64.as<double>();
+    d.rhs = b->rhs.as<double2>();
+    d.dx = b->dx.as<double2>();
+    d.res = b->res.as<double2>();
+    d.X = b->X.p;
+    d.mis_bits = b->mis.as<unsigned long long>();
+    d.state = b->state.as<int>();
+    d.solving = b->solving.as<int>();
+    d.singular = b->singular.as<int>();
+    d.iters = b->iters.as<int>();
+    d.status = b->status.as<int>();
+    d.final_mis = b->fmis.as<double>();
+    d.gsolve = b->gsolve.as<int>();
+    d.giter = b->giter.as<int>();
+    d.ctrl = b->ctrl.as<int>();
+    d.tol = b->tol.as<double>();
+    *out = b.release();
+    return GAPK_OK;
+}
+
+int gapk_nr_batch_destroy(gapk_nr_batch b) {
+    delete b;
+    return GAPK_OK;
+}
+
+int64_t gapk_nr_batch_device_bytes(gapk_nr_batch b) {
+    if (!b) return 0;
+    int64_t s = 0;
+    for (DevBuf* d : {&b->V, &b->Sspec, &b->Scalc, &b->Y, &b->F, &b->A64, &b->rhs, &b->dx,
+                      &b->res, &b->X, &b->mis, &b->state, &b->solving, &b->singular, &b->iters,
+                      &b->status, &b->fmis, &b->gsolve, &b->giter, &b->ctrl, &b->tol})
+        s += static_cast<int64_t>(d->bytes);
+    return s;
+}
+
+int gapk_nr_solve(gapk_nr_batch b, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
+                  void* stream) {
+    if (!b) {
+        set_error("gapk_nr_solve: null batch");
+        return GAPK_EINVAL;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = load_inputs(b, in, st);
+    if (rc) return rc;
+    if (in->max_iterations > 0) {
+        if (b->use_graph) {
+            rc = build_graph(b, st);
+            if (rc) return rc;
+            GAPK_CUDA_TRY(cudaGraphLaunch(b->exec, st));
+        } else {
+            // host-driven loop: one synchronisation per iteration
+            for (int it = 0; it < in->max_iterations; ++it) {
+                dispatch_tsw<BodyOp>(b->precision, b->sw, b, st, 0,
+                                     cudaGraphConditionalHandle{});
+                rc = check_launch();
+                if (rc) return rc;
+                int any = 0;
+                GAPK_CUDA_TRY(cudaMemcpyAsync(&any, b->dev.ctrl + 2, sizeof(int),
+                                              cudaMemcpyDeviceToHost, st));
+                GAPK_CUDA_TRY(cudaStreamSynchronize(st));
+                if (!any) break;
+            }
+        }
+    }
+    if (out) {
+        dispatch_tsw<StoreOp>(b->precision, b->sw, b, out, st);
+        rc = check_launch();
+        if (rc) return rc;
+    }
+    return GAPK_OK;
+}
+
+int gapk_nr_last_loop_count(gapk_nr_batch b, void* stream, int* h_loops) {
+    if (!b || !h_loops) return GAPK_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    GAPK_CUDA_TRY(cudaMemcpyAsync(h_loops, b->dev.ctrl + 4, sizeof(int), cudaMemcpyDeviceToHost,
+                                  st));
+    GAPK_CUDA_TRY(cudaStreamSynchronize(st));
+    return GAPK_OK;
+}
+
+int gapk_nr_stage_load(gapk_nr_batch b, const gapk_nr_inputs* in, void* stream) {
+    if (!b) return GAPK_EINVAL;
+    return load_inputs(b, in, static_cast<cudaStream_t>(stream));
+}
+
+static int stage(gapk_nr_batch b, int which, void* stream) {
+    if (!b) {
+        set_error("stage: null batch");
+        return GAPK_EINVAL;
+    }
+    dispatch_tsw<StageOp>(b->precision, b->sw, b, which, static_cast<cudaStream_t>(stream));
+    return check_launch();
+}
+int gapk_nr_stage_mismatch(gapk_nr_batch b, void* s) { return stage(b, 0, s); }
+int gapk_nr_stage_jacobian(gapk_nr_batch b, void* s) { return stage(b, 1, s); }
+int gapk_nr_stage_factor(gapk_nr_batch b, void* s) { return stage(b, 2, s); }
+int gapk_nr_stage_solve(gapk_nr_batch b, void* s) { return stage(b, 3, s); }
+
+int gapk_nr_stage_get_correction(gapk_nr_batch b, double* d_dx, void* stream) {
+    if (!b || !d_dx) return GAPK_EINVAL;
+    dispatch_tsw<ToRefOp>(b->precision, b->sw, b, b->dev.dx, b->plan->d_var.as<int>(),
+                          b->plan->h.n_vars, 1.0, d_dx, static_cast<cudaStream_t>(stream));
+    return check_launch();
+}
+
+int gapk_nr_stage_get_mismatch(gapk_nr_batch b, double* d_f, void* stream) {
+    if (!b || !d_f) return GAPK_EINVAL;
+    dispatch_tsw<ToRefOp>(b->precision, b->sw, b, b->dev.rhs, b->plan->d_eq.as<int>(),
+                          b->plan->h.n_vars, -1.0, d_f, static_cast<cudaStream_t>(stream));
+    return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,544 @@
+// Device kernels of the Newton-Raphson loop.
+//
+// Layout: scenarios sharing one plan are packed in groups of SW ("lanes"); every per-bus,
+// per-node and per-slot quantity is stored [group][item][lane], so the SW threads that
+// handle the same item for the SW scenarios of a group touch one contiguous run of memory
+// (SW*16 B for a complex FP64 value, SW*16 B for an FP32 2x2 block).  Index lists (CSR of
+// Y, factor schedule) are shared by all lanes and read once per warp.
+//
+// Reference semantics restated (src/solver/powerflow/cpu/cpu_newton_raphson.cpp):
+//   mismatch   :243-337  S = V conj(Y V), Delta = S - S_spec, P rows for non-slack buses, Q
+//                        rows for PQ buses, converged when max |Delta| < tol (:115-157)
+//   Jacobian   :546-727  polar partial derivatives; |V| < 1e-6 replaced by 1 (:578)
+//   update     :438-504  damped (0.9) and clamped polar update (policy REFERENCE)
+#pragma once
+#include <cuda_runtime.h>
+
+#include "blocks.cuh"
+
+namespace gapk {
+
+enum { BUS_PQ = 0, BUS_PV = 1, BUS_SLACK = 2 };
+enum { SC_CONVERGED = 0, SC_MAXITER = 1, SC_SINGULAR = 2, SC_NONFINITE = 3 };
+
+struct PlanDev {
+    int n_bus, nb, nnz_y, n_slots, nnz_l, n_levels, n_a;
+    int jac_mode;  // 0: reference (last duplicate, |x| <= 1e-12 dropped), 1: exact
+    const int* y_row_ptr;
+    const int* y_col;
+    const int* bus_type;
+    const int* node_of_bus;
+    const int4* slot_info;
+    const int* slot_src;
+    const int* slot_a;
+    const int* level_ptr;
+    const int* level_nodes;
+    const int* fa_ptr;
+    const int4* targets;
+    const int2* pairs;
+    const int* fb_ptr;
+    const int2* scale;
+    const int* lptr;
+    const int* lidx;
+    const int* rptr;
+    const int2* rlist;
+    const int* arow_ptr;
+    const int2* arow;
+};
+
+// Per-batch device state.  q = group*SW + lane indexes per-scenario arrays.
+struct BatchDev {
+    int n_scen, n_groups, sw, y_shared;
+    double2* V;       // [G][n_bus][SW]
+    double2* Sspec;   // [G][n_bus][SW]
+    double2* Scalc;   // [G][n_bus][SW]
+    double2* Y;       // [nnz] (shared) or [G][nnz][SW]
+    void* F;          // factor blocks [G][n_slots][SW]
+    double* A64;      // FP64 Jacobian blocks [G][n_a][SW][4] (iterative refinement) or null
+    double2* rhs;     // -Delta per node [G][nb][SW]
+    double2* dx;      // Newton correction per node [G][nb][SW]
+    double2* res;     // refinement residual [G][nb][SW]
+    void* X;          // triangular-solve work vector [G][nb][SW] (T2)
+    unsigned long long* mis_bits;  // [G*SW] max |Delta| bits of the current iteration
+    int* state;       // [G*SW] 0 iterating, 1 done
+    int* solving;     // [G*SW] correction + update this iteration
+    int* singular;    // [G*SW]
+    int* iters;       // [G*SW]
+    int* status;      // [G*SW]
+    double* final_mis;  // [G*SW]
+    int* gsolve;      // [G]
+    int* giter;       // [G]
+    int* ctrl;        // [0] iteration, [1] max_iter, [2] any iterating, [3] policy, [4] loops
+    double* tol;      // [1]
+};
+
+// ---------------------------------------------------------------------------------------
+// load: interleave inputs, flat start, reset state
+// ---------------------------------------------------------------------------------------
+template <int SW>
+__global__ void k_load(PlanDev P, BatchDev B, const double2* __restrict__ y_in,
+                       const double2* __restrict__ s_in, const double2* __restrict__ v_in,
+                       const double* __restrict__ u_pu) {
+    const int g = blockIdx.y;
+    const int n = P.n_bus;
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(tid / SW), lane = (int)(tid % SW);
+    int q = g * SW + lane;
+    int src = q < B.n_scen ? q : g * SW;  // padding lanes mirror the group's first scenario
+    if (i < n) {
+        size_t o = ((size_t)g * n + i) * SW + lane;
+        B.Sspec[o] = s_in[(size_t)src * n + i];
+        double2 v;
+        if (v_in) {
+            v = v_in[(size_t)src * n + i];
+        } else {
+            // flat start (cpu_newton_raphson.cpp:77-88): SLACK/PV at u_pu, PQ at 0.98, angle 0
+            int t = P.bus_type[i];
+            double m = (t == BUS_PQ) ? 0.98 : (u_pu ? u_pu[i] : 1.0);
+            v = make_double2(m, 0.0);
+        }
+        B.V[o] = v;
+    }
+    if (i < n) {
+        if (!B.y_shared) {
+            for (int p = i; p < P.nnz_y; p += n)
+                B.Y[((size_t)g * P.nnz_y + p) * SW + lane] = y_in[(size_t)src * P.nnz_y + p];
+        } else if (g == 0 && lane == 0) {
+            for (int p = i; p < P.nnz_y; p += n) B.Y[p] = y_in[p];
+        }
+    }
+    if (i == 0) {
+        B.mis_bits[q] = 0ull;
+        B.state[q] = q < B.n_scen ? 0 : 1;
+        B.solving[q] = q < B.n_scen ? 1 : 0;
+        B.singular[q] = 0;
+        B.iters[q] = 0;
+        B.status[q] = SC_MAXITER;
+        B.final_mis[q] = 0.0;
+        if (lane == 0) {
+            B.gsolve[g] = 1;
+            B.giter[g] = 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// mismatch: fused Y*V SpMV, S = V conj(I), Delta, rhs, per-scenario max |Delta|
+// ---------------------------------------------------------------------------------------
+template <int SW>
+__global__ void __launch_bounds__(256) k_mismatch(PlanDev P, BatchDev B) {
+    const int g = blockIdx.y;
+    if (!B.giter[g]) return;
+    const int n = P.n_bus;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = tid / SW, lane = tid % SW;
+    double m = 0.0;
+    if (i < n) {
+        const double2* Vg = B.V + (size_t)g * n * SW;
+        const int pb = P.y_row_ptr[i], pe = P.y_row_ptr[i + 1];
+        double ir = 0.0, ii = 0.0;
+        if (B.y_shared) {
+            for (int p = pb; p < pe; ++p) {
+                const double2 y = B.Y[p];
+                const double2 v = Vg[(size_t)P.y_col[p] * SW + lane];
+                ir = fma(y.x, v.x, ir);
+                ir = fma(-y.y, v.y, ir);
+                ii = fma(y.x, v.y, ii);
+                ii = fma(y.y, v.x, ii);
+            }
+        } else {
+            const double2* Yg = B.Y + (size_t)g * P.nnz_y * SW;
+            for (int p = pb; p < pe; ++p) {
+                const double2 y = Yg[(size_t)p * SW + lane];
+                const double2 v = Vg[(size_t)P.y_col[p] * SW + lane];
+                ir = fma(y.x, v.x, ir);
+                ir = fma(-y.y, v.y, ir);
+                ii = fma(y.x, v.y, ii);
+                ii = fma(y.y, v.x, ii);
+            }
+        }
+        const size_t o = ((size_t)g * n + i) * SW + lane;
+        const double2 vi = Vg[(size_t)i * SW + lane];
+        // S = V conj(I)
+        const double2 s = make_double2(fma(vi.x, ir, vi.y * ii), fma(vi.y, ir, -vi.x * ii));
+        B.Scalc[o] = s;
+        const int t = P.bus_type[i];
+        if (t != BUS_SLACK) {
+            const double2 sp = B.Sspec[o];
+            const double dp = s.x - sp.x;
+            const double dq = (t == BUS_PQ) ? s.y - sp.y : 0.0;
+            const int node = P.node_of_bus[i];
+            B.rhs[((size_t)g * P.nb + node) * SW + lane] = make_double2(-dp, -dq);
+            m = nmax(fabs(dp), fabs(dq));
+        }
+    }
+#pragma unroll
+    for (int off = SW; off < 32; off <<= 1) m = nmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) < SW && m != 0.0) {
+        atomicMax(&B.mis_bits[g * SW + lane], (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// convergence test and loop control (one CTA)
+// ---------------------------------------------------------------------------------------
+template <int SW>
+__global__ void k_check(BatchDev B, int use_cond, cudaGraphConditionalHandle handle) {
+    __shared__ int any_iter;
+    if (threadIdx.x == 0) any_iter = 0;
+    __syncthreads();
+    const int it = B.ctrl[0];
+    const int max_iter = B.ctrl[1];
+    const double tol = B.tol[0];
+    const int total = B.n_groups * SW;
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        if (q >= B.n_scen || B.state[q] != 0) {
+            B.solving[q] = 0;
+            continue;
+        }
+        const double m = __longlong_as_double((long long)B.mis_bits[q]);
+        B.mis_bits[q] = 0ull;
+        B.final_mis[q] = m;
+        if (!isfinite(m)) {
+            B.state[q] = 1;
+            B.status[q] = SC_NONFINITE;
+            B.iters[q] = it + 1;
+            B.solving[q] = 0;
+        } else if (m < tol) {
+            B.state[q] = 1;
+            B.status[q] = SC_CONVERGED;
+            B.iters[q] = it + 1;
+            B.solving[q] = 0;
+        } else {
+            B.solving[q] = 1;
+            if (it + 1 >= max_iter) {
+                B.state[q] = 1;
+                B.status[q] = SC_MAXITER;
+                B.iters[q] = max_iter;
+            }
+        }
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < B.n_groups; g += blockDim.x) {
+        int sv = 0, iv = 0;
+        for (int l = 0; l < SW; ++l) {
+            const int q = g * SW + l;
+            if (q < B.n_scen) {
+                sv |= B.solving[q];
+                iv |= (B.state[q] == 0);
+            }
+        }
+        B.gsolve[g] = sv;
+        B.giter[g] = iv;
+        if (iv) atomicOr(&any_iter, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        B.ctrl[0] = it + 1;
+        B.ctrl[2] = any_iter;
+        B.ctrl[4] = it + 1;
+        if (use_cond) cudaGraphSetConditional(handle, any_iter ? 1u : 0u);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Jacobian value fill on the fixed factor pattern (fill-in slots are zeroed)
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void polar_parts(double2 v, double& vmr, double& c, double& s) {
+    const double vm = hypot(v.x, v.y);
+    if (vm > 0.0) {
+        c = v.x / vm;
+        s = v.y / vm;
+    } else {
+        c = 1.0;
+        s = 0.0;
+    }
+    vmr = vm < 1e-6 ? 1.0 : vm;
+}
+
+template <typename T, int SW>
+__global__ void __launch_bounds__(256) k_jfill(PlanDev P, BatchDev B) {
+    const int g = blockIdx.y;
+    if (!B.gsolve[g]) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = tid / SW, lane = tid % SW;
+    if (slot >= P.n_slots) return;
+    const int4 si = P.slot_info[slot];
+    const int n = P.n_bus;
+    Blk<double> J = {0.0, 0.0, 0.0, 0.0};
+    const bool diag = si.x == si.y;
+    if (diag || si.z < si.w) {
+        double G = 0.0, Bv = 0.0;
+        for (int e = si.z; e < si.w; ++e) {
+            const int p = P.slot_src[e];
+            const double2 y = B.y_shared ? B.Y[p] : B.Y[((size_t)g * P.nnz_y + p) * SW + lane];
+            G += y.x;
+            Bv += y.y;
+        }
+        const double2* Vg = B.V + (size_t)g * n * SW;
+        const bool pqi = P.bus_type[si.x] == BUS_PQ;
+        double vmi, ci, sni;
+        polar_parts(Vg[(size_t)si.x * SW + lane], vmi, ci, sni);
+        if (diag) {
+            const double2 S = B.Scalc[((size_t)g * n + si.x) * SW + lane];
+            J.a = -S.y - Bv * vmi * vmi;
+            J.b = S.x / vmi + G * vmi;
+            J.c = S.x - G * vmi * vmi;
+            J.d = S.y / vmi - Bv * vmi;
+            if (!pqi) {
+                J.b = 0.0;
+                J.c = 0.0;
+                J.d = 1.0;
+            }
+        } else {
+            const bool pqj = P.bus_type[si.y] == BUS_PQ;
+            double vmj, cj, snj;
+            polar_parts(Vg[(size_t)si.y * SW + lane], vmj, cj, snj);
+            // u = |V_i| e^{j(theta_i - theta_j)}
+            const double uc = vmi * (ci * cj + sni * snj);
+            const double ud = vmi * (sni * cj - ci * snj);
+            const double gcbd = G * uc + Bv * ud;
+            const double gdbc = G * ud - Bv * uc;
+            J.a = vmj * gdbc;
+            J.b = gcbd;
+            J.c = -vmj * gcbd;
+            J.d = gdbc;
+            if (!pqi) {
+                J.c = 0.0;
+                J.d = 0.0;
+            }
+            if (!pqj) {
+                J.b = 0.0;
+                J.d = 0.0;
+            }
+        }
+    }
+    if (P.jac_mode == 0) {
+        // convert_to_sparse_matrix drops |x| <= 1e-12 (cpu_newton_raphson.cpp:754)
+        if (fabs(J.a) <= 1e-12) J.a = 0.0;
+        if (fabs(J.b) <= 1e-12) J.b = 0.0;
+        if (fabs(J.c) <= 1e-12) J.c = 0.0;
+        if (fabs(J.d) <= 1e-12 && !(diag && J.d == 1.0)) J.d = 0.0;
+    }
+    Blk<T>* F = reinterpret_cast<Blk<T>*>(B.F) + ((size_t)g * P.n_slots + slot) * SW + lane;
+    stb(F, Blk<T>{(T)J.a, (T)J.b, (T)J.c, (T)J.d});
+    if (B.A64) {
+        const int a = P.slot_a[slot];
+        if (a >= 0) {
+            Blk<double>* A = reinterpret_cast<Blk<double>*>(B.A64) +
+                             ((size_t)g * P.n_a + a) * SW + lane;
+            stb(A, J);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// numeric block LU (left-looking Crout), one CTA per group, level by level
+// ---------------------------------------------------------------------------------------
+template <typename T, int SW>
+__global__ void k_factor(PlanDev P, BatchDev B) {
+    const int g = blockIdx.x;
+    if (!B.gsolve[g]) return;
+    Blk<T>* F = reinterpret_cast<Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
+    const int lane = threadIdx.x % SW;
+    const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
+    bool bad = false;
+    for (int h = 0; h < P.n_levels; ++h) {
+        const int ta = P.fa_ptr[h], tb = P.fa_ptr[h + 1];
+        for (int t = ta + e0; t < tb; t += ne) {
+            const int4 tg = P.targets[t];
+            Blk<T> acc = ldb(F + (size_t)tg.x * SW + lane);
+            for (int p = tg.y; p < tg.z; ++p) {
+                const int2 pr = P.pairs[p];
+                msub(acc, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
+            }
+            if (tg.w) {
+                bool ok;
+                acc = inv2(acc, ok);
+                bad |= !ok;
+            }
+            stb(F + (size_t)tg.x * SW + lane, acc);
+        }
+        __syncthreads();
+        const int sa = P.fb_ptr[h], sb = P.fb_ptr[h + 1];
+        if (sb > sa) {
+            for (int t = sa + e0; t < sb; t += ne) {
+                const int2 sc = P.scale[t];
+                Blk<T>* Lp = F + (size_t)sc.x * SW + lane;
+                stb(Lp, mul(ldb(Lp), ldb(F + (size_t)sc.y * SW + lane)));
+            }
+            __syncthreads();
+        }
+    }
+    if (bad) B.singular[g * SW + lane] = 1;
+}
+
+// ---------------------------------------------------------------------------------------
+// triangular solves: L y = b (unit lower), U x = y; x written as FP64 (optionally added)
+// ---------------------------------------------------------------------------------------
+template <typename T, int SW>
+__global__ void k_solve(PlanDev P, BatchDev B, const double2* __restrict__ rhs, double2* out,
+                        int accumulate) {
+    const int g = blockIdx.x;
+    if (!B.gsolve[g]) return;
+    const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
+    Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
+    const double2* R = rhs + (size_t)g * P.nb * SW;
+    double2* O = out + (size_t)g * P.nb * SW;
+    const int lane = threadIdx.x % SW;
+    const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
+    const int L = P.n_levels;
+    for (int h = 0; h < L; ++h) {
+        for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
+            const int k = P.level_nodes[t];
+            const double2 b = R[(size_t)k * SW + lane];
+            Vec2<T> acc = {(T)b.x, (T)b.y};
+            for (int q = P.rptr[k]; q < P.rptr[k + 1]; ++q) {
+                const int2 r = P.rlist[q];
+                msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
+            }
+            stv(X + (size_t)k * SW + lane, acc);
+        }
+        __syncthreads();
+    }
+    const int Ub = P.nb + P.nnz_l;
+    for (int h = L - 1; h >= 0; --h) {
+        for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
+            const int k = P.level_nodes[t];
+            Vec2<T> acc = ldv(X + (size_t)k * SW + lane);
+            for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
+                msubv(acc, ldb(F + (size_t)(Ub + p) * SW + lane),
+                      ldv(X + (size_t)P.lidx[p] * SW + lane));
+            }
+            const Vec2<T> x = mulv(ldb(F + (size_t)k * SW + lane), acc);
+            stv(X + (size_t)k * SW + lane, x);
+            double2* o = O + (size_t)k * SW + lane;
+            if (accumulate) {
+                const double2 old = *o;
+                *o = make_double2(old.x + (double)x.x, old.y + (double)x.y);
+            } else {
+                *o = make_double2((double)x.x, (double)x.y);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// refinement residual: res = rhs - J dx with the FP64 Jacobian blocks
+template <int SW>
+__global__ void __launch_bounds__(256) k_residual(PlanDev P, BatchDev B) {
+    const int g = blockIdx.y;
+    if (!B.gsolve[g]) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = tid / SW, lane = tid % SW;
+    if (k >= P.nb) return;
+    const size_t base = (size_t)g * P.nb * SW;
+    const double2 b = B.rhs[base + (size_t)k * SW + lane];
+    Vec2<double> acc = {b.x, b.y};
+    const Blk<double>* A = reinterpret_cast<const Blk<double>*>(B.A64) + (size_t)g * P.n_a * SW;
+    for (int e = P.arow_ptr[k]; e < P.arow_ptr[k + 1]; ++e) {
+        const int2 ac = P.arow[e];
+        const double2 x = B.dx[base + (size_t)ac.y * SW + lane];
+        msubv(acc, ldb(A + (size_t)ac.x * SW + lane), Vec2<double>{x.x, x.y});
+    }
+    B.res[base + (size_t)k * SW + lane] = make_double2(acc.x, acc.y);
+}
+
+// ---------------------------------------------------------------------------------------
+// voltage update
+// ---------------------------------------------------------------------------------------
+template <int SW>
+__global__ void __launch_bounds__(256) k_update(PlanDev P, BatchDev B) {
+    const int g = blockIdx.y;
+    if (!B.gsolve[g]) return;
+    const int n = P.n_bus;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = tid / SW, lane = tid % SW;
+    if (i >= n) return;
+    const int q = g * SW + lane;
+    const bool real = q < B.n_scen;
+    if (real) {
+        if (B.singular[q]) {
+            // the reference keeps V unchanged when factorize() fails and runs to max_iter
+            if (i == 0 && B.solving[q]) {
+                B.state[q] = 1;
+                B.status[q] = SC_SINGULAR;
+                B.iters[q] = B.ctrl[1];
+                B.solving[q] = 0;
+            }
+            return;
+        }
+        if (!B.solving[q]) return;
+    }
+    const int node = P.node_of_bus[i];
+    if (node < 0) return;
+    const double2 d = B.dx[((size_t)g * P.nb + node) * SW + lane];
+    const size_t o = ((size_t)g * n + i) * SW + lane;
+    double2 v = B.V[o];
+    const bool pq = P.bus_type[i] == BUS_PQ;
+    if (B.ctrl[3] == 0) {
+        // reference policy (cpu_newton_raphson.cpp:457-503)
+        const double vm = hypot(v.x, v.y);
+        double a = 0.9 * d.x;
+        if (fabs(a) > 0.15) a = 0.15 * (a > 0 ? 1.0 : -1.0);
+        double sn, cs;
+        sincos(atan2(v.y, v.x) + a, &sn, &cs);
+        v = make_double2(vm * cs, vm * sn);
+        if (pq) {
+            const double vm0 = hypot(v.x, v.y);
+            double c = 0.9 * d.y;
+            if (fabs(c) > 0.08) c = 0.08 * (c > 0 ? 1.0 : -1.0);
+            double vmn = vm0 + c;
+            vmn = (vmn < 0.5) ? 0.5 : vmn;
+            vmn = (1.5 < vmn) ? 1.5 : vmn;
+            sincos(atan2(v.y, v.x), &sn, &cs);
+            v = make_double2(vmn * cs, vmn * sn);
+        }
+    } else {
+        double vm = hypot(v.x, v.y);
+        const double va = atan2(v.y, v.x) + d.x;
+        if (pq) vm += d.y;
+        double sn, cs;
+        sincos(va, &sn, &cs);
+        v = make_double2(vm * cs, vm * sn);
+    }
+    B.V[o] = v;
+}
+
+// ---------------------------------------------------------------------------------------
+// results out (scenario-major) and reference-order views of the stage vectors
+// ---------------------------------------------------------------------------------------
+template <int SW>
+__global__ void k_store(PlanDev P, BatchDev B, double2* v_out, int* it_out, int* st_out,
+                        double* fm_out) {
+    const int n = P.n_bus;
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long total = (long)B.n_scen * n;
+    if (tid < total) {
+        const int s = (int)(tid / n), i = (int)(tid % n);
+        const int g = s / SW, lane = s % SW;
+        if (v_out) v_out[tid] = B.V[((size_t)g * n + i) * SW + lane];
+        if (i == 0) {
+            if (it_out) it_out[s] = B.iters[s];
+            if (st_out) st_out[s] = B.status[s];
+            if (fm_out) fm_out[s] = B.final_mis[s];
+        }
+    }
+}
+
+// node vector [G][nb][SW] -> reference order [n_scen][n_vars]; map[node*2+c] gives the
+// reference index (or -1); sign multiplies the value
+template <int SW>
+__global__ void k_node_to_ref(const double2* __restrict__ src, int nb, int n_scen, int n_vars,
+                              const int* __restrict__ map, double sign, double* dst) {
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long)n_scen * nb) return;
+    const int s = (int)(tid / nb), k = (int)(tid % nb);
+    const int g = s / SW, lane = s % SW;
+    const double2 v = src[((size_t)g * nb + k) * SW + lane];
+    const int a = map[2 * k], b = map[2 * k + 1];
+    if (a >= 0) dst[(size_t)s * n_vars + a] = sign * v.x;
+    if (b >= 0) dst[(size_t)s * n_vars + b] = sign * v.y;
+}
+
+}  // namespace gapk

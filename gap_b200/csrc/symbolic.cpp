@@ -1,0 +1,436 @@
+// Host-side analysis, run once per topology:
+//   * the Y-bus CSR pattern in the reference's triplet order
+//     (src/admittance/cpu/cpu_admittance_matrix.cpp:100-186), with per-slot sources and the
+//     per-bus diagonal contribution lists for the device's segmented reduction;
+//   * the Newton-Raphson plan: 2x2-block Jacobian pattern on the non-slack buses, a
+//     minimum-degree elimination order, the symbolic block factorisation (elimination graph),
+//     the elimination-tree level schedule and all index lists the device kernels walk.
+#include <algorithm>
+#include <cstdint>
+#include <numeric>
+#include <set>
+#include <stdexcept>
+#include <utility>
+
+#include "internal.h"
+
+namespace gapk {
+
+void build_ybus_pattern(int n_bus, int n_branch, const int* from, const int* to,
+                        const int* in_service, int n_shunt, const int* shunt_bus,
+                        YbusPatternHost& out) {
+    struct Trip {
+        int row, col, src;
+    };
+    std::vector<Trip> trips;
+    trips.reserve(static_cast<size_t>(n_bus) + 2 * static_cast<size_t>(n_branch));
+    auto valid = [&](int b) {
+        return in_service[b] != 0 && from[b] >= 0 && from[b] < n_bus && to[b] >= 0 &&
+               to[b] < n_bus;
+    };
+    // off-diagonal triplets in branch order (cpu_admittance_matrix.cpp:138-139)
+    for (int b = 0; b < n_branch; ++b) {
+        if (!valid(b)) continue;
+        trips.push_back({from[b], to[b], 2 * b});
+        trips.push_back({to[b], from[b], 2 * b + 1});
+    }
+    // diagonal triplets last (cpu_admittance_matrix.cpp:143-145)
+    for (int i = 0; i < n_bus; ++i) trips.push_back({i, i, -(i + 1)});
+    std::stable_sort(trips.begin(), trips.end(), [](Trip const& a, Trip const& b) {
+        if (a.row != b.row) return a.row < b.row;
+        return a.col < b.col;
+    });
+    out.n_bus = n_bus;
+    out.n_branch = n_branch;
+    out.n_shunt = n_shunt;
+    out.nnz = static_cast<int>(trips.size());
+    out.row_ptr.assign(n_bus + 1, 0);
+    out.col_idx.resize(trips.size());
+    out.slot_src.resize(trips.size());
+    for (size_t p = 0; p < trips.size(); ++p) {
+        out.row_ptr[trips[p].row + 1]++;
+        out.col_idx[p] = trips[p].col;
+        out.slot_src[p] = trips[p].src;
+    }
+    for (int i = 0; i < n_bus; ++i) out.row_ptr[i + 1] += out.row_ptr[i];
+    // diagonal accumulation order: shunts (appliance order, :88-97), then branch ends in branch
+    // order, from end before to end (:134-135)
+    std::vector<int> cnt(n_bus + 1, 0);
+    for (int s = 0; s < n_shunt; ++s)
+        if (shunt_bus[s] >= 0 && shunt_bus[s] < n_bus) cnt[shunt_bus[s] + 1]++;
+    for (int b = 0; b < n_branch; ++b) {
+        if (!valid(b)) continue;
+        cnt[from[b] + 1]++;
+        cnt[to[b] + 1]++;
+    }
+    for (int i = 0; i < n_bus; ++i) cnt[i + 1] += cnt[i];
+    out.diag_ptr = cnt;
+    out.diag_src.assign(cnt[n_bus], 0);
+    std::vector<int> fillp(cnt.begin(), cnt.end() - 1);
+    for (int s = 0; s < n_shunt; ++s)
+        if (shunt_bus[s] >= 0 && shunt_bus[s] < n_bus) out.diag_src[fillp[shunt_bus[s]]++] = -(s + 1);
+    for (int b = 0; b < n_branch; ++b) {
+        if (!valid(b)) continue;
+        out.diag_src[fillp[from[b]]++] = 2 * b;
+        out.diag_src[fillp[to[b]]++] = 2 * b + 1;
+    }
+}
+
+namespace {
+
+// Elimination on the quotient-free elimination graph.  Returns the elimination order (as
+// indices into the node list) and, per eliminated node, its neighbour set at elimination
+// (= the strictly-lower structure of its column of L).  Minimum degree, ties broken by the
+// lower index, so the result is deterministic.
+void eliminate(int nq, std::vector<std::vector<int>>& adj, bool mindeg, std::vector<int>& order,
+               std::vector<std::vector<int>>& structq) {
+    order.clear();
+    order.reserve(nq);
+    structq.assign(nq, {});
+    std::vector<char> done(nq, 0);
+    std::set<std::pair<int, int>> pq;
+    if (mindeg)
+        for (int q = 0; q < nq; ++q) pq.insert({static_cast<int>(adj[q].size()), q});
+    std::vector<int> tmp;
+    for (int step = 0; step < nq; ++step) {
+        int v;
+        if (mindeg) {
+            v = pq.begin()->second;
+            pq.erase(pq.begin());
+        } else {
+            v = step;
+        }
+        done[v] = 1;
+        order.push_back(v);
+        std::vector<int> nbrs = std::move(adj[v]);
+        adj[v].clear();
+        for (int u : nbrs) {
+            if (mindeg) pq.erase({static_cast<int>(adj[u].size()), u});
+            tmp.clear();
+            std::set_union(adj[u].begin(), adj[u].end(), nbrs.begin(), nbrs.end(),
+                           std::back_inserter(tmp));
+            adj[u].clear();
+            for (int w : tmp)
+                if (w != u && w != v) adj[u].push_back(w);
+            if (mindeg) pq.insert({static_cast<int>(adj[u].size()), u});
+        }
+        structq[v] = std::move(nbrs);
+    }
+}
+
+inline int find_in(std::vector<int> const& lidx, int b, int e, int x) {
+    auto it = std::lower_bound(lidx.begin() + b, lidx.begin() + e, x);
+    if (it == lidx.begin() + e || *it != x) return -1;
+    return static_cast<int>(it - lidx.begin());
+}
+
+}  // namespace
+
+bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx,
+                const int* bus_type, int jac_mode, int ordering, NRPlanHost& P) {
+    P = NRPlanHost{};
+    P.n_bus = n_bus;
+    P.nnz_y = nnz_y;
+    P.jac_mode = jac_mode;
+    P.bus_type.assign(bus_type, bus_type + n_bus);
+    if (y_row_ptr[0] != 0 || y_row_ptr[n_bus] != nnz_y) {
+        set_error("Y row_ptr inconsistent with nnz");
+        return false;
+    }
+    for (int i = 0; i < n_bus; ++i) {
+        if (y_row_ptr[i + 1] < y_row_ptr[i]) {
+            set_error("Y row_ptr not monotone");
+            return false;
+        }
+        int t = bus_type[i];
+        if (t < 0 || t > 2) {
+            set_error("bus_type must be 0 (PQ), 1 (PV) or 2 (SLACK)");
+            return false;
+        }
+        if (t == 2) P.n_slack++;
+        if (t == 1) P.n_pv++;
+        if (t == 0) P.n_pq++;
+    }
+    for (int p = 0; p < nnz_y; ++p) {
+        if (y_col_idx[p] < 0 || y_col_idx[p] >= n_bus) {
+            set_error("Y col_idx out of range");
+            return false;
+        }
+    }
+    P.n_vars = (n_bus - P.n_slack) + P.n_pq;
+
+    // node candidates: non-slack buses in bus order (q index)
+    std::vector<int> q_of_bus(n_bus, -1), bus_of_q;
+    for (int i = 0; i < n_bus; ++i)
+        if (bus_type[i] != 2) {
+            q_of_bus[i] = static_cast<int>(bus_of_q.size());
+            bus_of_q.push_back(i);
+        }
+    const int nb = static_cast<int>(bus_of_q.size());
+    P.nb = nb;
+
+    // symmetrised block graph
+    std::vector<std::vector<int>> adj(nb);
+    for (int i = 0; i < n_bus; ++i) {
+        int qi = q_of_bus[i];
+        if (qi < 0) continue;
+        for (int p = y_row_ptr[i]; p < y_row_ptr[i + 1]; ++p) {
+            int qj = q_of_bus[y_col_idx[p]];
+            if (qj < 0 || qj == qi) continue;
+            adj[qi].push_back(qj);
+            adj[qj].push_back(qi);
+        }
+    }
+    for (auto& a : adj) {
+        std::sort(a.begin(), a.end());
+        a.erase(std::unique(a.begin(), a.end()), a.end());
+    }
+
+    std::vector<int> order;
+    std::vector<std::vector<int>> structq;
+    eliminate(nb, adj, ordering == 0, order, structq);
+
+    std::vector<int> node_of_q(nb);
+    for (int k = 0; k < nb; ++k) node_of_q[order[k]] = k;
+    P.node_of_bus.assign(n_bus, -1);
+    P.bus_of_node.resize(nb);
+    P.node_pq.resize(nb);
+    for (int k = 0; k < nb; ++k) {
+        int bus = bus_of_q[order[k]];
+        P.bus_of_node[k] = bus;
+        P.node_of_bus[bus] = k;
+        P.node_pq[k] = bus_type[bus] == 0 ? 1 : 0;
+    }
+    // column structures
+    P.lptr.assign(nb + 1, 0);
+    for (int k = 0; k < nb; ++k) P.lptr[k + 1] = P.lptr[k] + static_cast<int>(structq[order[k]].size());
+    P.nnz_l = P.lptr[nb];
+    P.lidx.resize(P.nnz_l);
+    for (int k = 0; k < nb; ++k) {
+        auto& s = structq[order[k]];
+        int b = P.lptr[k];
+        for (size_t t = 0; t < s.size(); ++t) P.lidx[b + t] = node_of_q[s[t]];
+        std::sort(P.lidx.begin() + b, P.lidx.begin() + P.lptr[k + 1]);
+    }
+    structq.clear();
+    const int nnzl = P.nnz_l;
+    P.n_slots = nb + 2 * nnzl;
+    const int Lbase = nb, Ubase = nb + nnzl;
+
+    // elimination tree heights -> levels
+    std::vector<int> height(nb, 0);
+    for (int k = 0; k < nb; ++k) {
+        if (P.lptr[k + 1] > P.lptr[k]) {
+            int parent = P.lidx[P.lptr[k]];
+            height[parent] = std::max(height[parent], height[k] + 1);
+        }
+    }
+    int nlev = nb ? (*std::max_element(height.begin(), height.end()) + 1) : 0;
+    P.n_levels = nlev;
+    P.node_level = height;
+    P.level_ptr.assign(nlev + 1, 0);
+    for (int k = 0; k < nb; ++k) P.level_ptr[height[k] + 1]++;
+    for (int h = 0; h < nlev; ++h) {
+        P.max_level_width = std::max(P.max_level_width, P.level_ptr[h + 1]);
+        P.level_ptr[h + 1] += P.level_ptr[h];
+    }
+    P.level_nodes.resize(nb);
+    {
+        std::vector<int> fp(P.level_ptr.begin(), P.level_ptr.end() - 1);
+        for (int k = 0; k < nb; ++k) P.level_nodes[fp[height[k]]++] = k;
+    }
+
+    // Y sources per (row bus, col bus): rows of (col, index), sorted by col then index
+    std::vector<std::pair<int, int>> yrow;
+    auto sources = [&](int i, int j, std::vector<int>& dst) {
+        // linear scan of row i (rows are short); keep order of appearance
+        int last = -1;
+        for (int p = y_row_ptr[i]; p < y_row_ptr[i + 1]; ++p) {
+            if (y_col_idx[p] != j) continue;
+            if (jac_mode == 0)
+                last = p;
+            else
+                dst.push_back(p);
+        }
+        if (jac_mode == 0 && last >= 0) dst.push_back(last);
+    };
+    P.slot_info.assign(static_cast<size_t>(P.n_slots) * 4, 0);
+    P.slot_src.clear();
+    std::vector<int> slot_a(P.n_slots, -1);
+    auto set_slot = [&](int slot, int rb, int cb) {
+        int b = static_cast<int>(P.slot_src.size());
+        sources(rb, cb, P.slot_src);
+        int e = static_cast<int>(P.slot_src.size());
+        P.slot_info[4 * slot + 0] = rb;
+        P.slot_info[4 * slot + 1] = cb;
+        P.slot_info[4 * slot + 2] = b;
+        P.slot_info[4 * slot + 3] = e;
+    };
+    for (int k = 0; k < nb; ++k) set_slot(k, P.bus_of_node[k], P.bus_of_node[k]);
+    for (int k = 0; k < nb; ++k)
+        for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
+            set_slot(Lbase + p, P.bus_of_node[P.lidx[p]], P.bus_of_node[k]);
+            set_slot(Ubase + p, P.bus_of_node[k], P.bus_of_node[P.lidx[p]]);
+        }
+    // A blocks: diagonal always, off-diagonal where Y has an entry; by block row
+    {
+        std::vector<std::vector<std::pair<int, int>>> rows(nb);  // (slot, col node)
+        for (int k = 0; k < nb; ++k) rows[k].push_back({k, k});
+        for (int k = 0; k < nb; ++k)
+            for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
+                int a = P.lidx[p];
+                int sl = Lbase + p, su = Ubase + p;
+                if (P.slot_info[4 * sl + 3] > P.slot_info[4 * sl + 2]) rows[a].push_back({sl, k});
+                if (P.slot_info[4 * su + 3] > P.slot_info[4 * su + 2]) rows[k].push_back({su, a});
+            }
+        P.arow_ptr.assign(nb + 1, 0);
+        P.arow.clear();
+        int na = 0;
+        for (int r = 0; r < nb; ++r) {
+            std::sort(rows[r].begin(), rows[r].end(),
+                      [](auto const& x, auto const& y) { return x.second < y.second; });
+            for (auto const& e : rows[r]) {
+                slot_a[e.first] = na;
+                P.arow.push_back(na);
+                P.arow.push_back(e.second);
+                ++na;
+            }
+            P.arow_ptr[r + 1] = na;
+        }
+        P.n_a = na;
+    }
+    P.slot_a = slot_a;
+    P.scale.clear();
+
+    // ---- numeric factorisation schedule (left-looking block Crout) ----
+    // Every node m contributes L(a,m) U(m,b) to target (a,b) for all a, b in struct(m).
+    std::vector<int64_t> cnt(P.n_slots + 1, 0);
+    auto target_of = [&](int a, int b) -> int {
+        if (a == b) return a;
+        if (a < b) {
+            int pos = find_in(P.lidx, P.lptr[a], P.lptr[a + 1], b);
+            return pos < 0 ? -1 : Ubase + pos;
+        }
+        int pos = find_in(P.lidx, P.lptr[b], P.lptr[b + 1], a);
+        return pos < 0 ? -1 : Lbase + pos;
+    };
+    for (int m = 0; m < nb; ++m) {
+        int b0 = P.lptr[m], e0 = P.lptr[m + 1];
+        for (int ia = b0; ia < e0; ++ia)
+            for (int ib = b0; ib < e0; ++ib) {
+                int t = target_of(P.lidx[ia], P.lidx[ib]);
+                if (t < 0) {
+                    set_error("symbolic factorisation inconsistent (missing fill slot)");
+                    return false;
+                }
+                cnt[t + 1]++;
+            }
+    }
+    for (int s = 0; s < P.n_slots; ++s) cnt[s + 1] += cnt[s];
+    P.n_pairs = cnt[P.n_slots];
+    std::vector<int> spairs(static_cast<size_t>(P.n_pairs) * 2);
+    {
+        std::vector<int64_t> fp(cnt.begin(), cnt.end() - 1);
+        for (int m = 0; m < nb; ++m) {
+            int b0 = P.lptr[m], e0 = P.lptr[m + 1];
+            for (int ia = b0; ia < e0; ++ia)
+                for (int ib = b0; ib < e0; ++ib) {
+                    int t = target_of(P.lidx[ia], P.lidx[ib]);
+                    int64_t q = fp[t]++;
+                    spairs[2 * q] = Lbase + ia;
+                    spairs[2 * q + 1] = Ubase + ib;
+                }
+        }
+    }
+    // group targets by owner level; phase A holds every slot (D, U row, L column) of the
+    // level's nodes, heaviest first; phase B scales the level's L columns by D^-1.
+    P.fa_ptr.assign(nlev + 1, 0);
+    P.fb_ptr.assign(nlev + 1, 0);
+    P.targets.clear();
+    P.pairs.clear();
+    P.pairs.reserve(spairs.size());
+    std::vector<int> lvl_slots;
+    for (int h = 0; h < nlev; ++h) {
+        lvl_slots.clear();
+        for (int t = P.level_ptr[h]; t < P.level_ptr[h + 1]; ++t) {
+            int k = P.level_nodes[t];
+            lvl_slots.push_back(k);
+            for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
+                lvl_slots.push_back(Ubase + p);
+                lvl_slots.push_back(Lbase + p);
+            }
+        }
+        std::stable_sort(lvl_slots.begin(), lvl_slots.end(), [&](int x, int y) {
+            return (cnt[x + 1] - cnt[x]) > (cnt[y + 1] - cnt[y]);
+        });
+        for (int s : lvl_slots) {
+            int pb = static_cast<int>(P.pairs.size() / 2);
+            for (int64_t q = cnt[s]; q < cnt[s + 1]; ++q) {
+                P.pairs.push_back(spairs[2 * q]);
+                P.pairs.push_back(spairs[2 * q + 1]);
+            }
+            int pe = static_cast<int>(P.pairs.size() / 2);
+            P.targets.push_back(s);
+            P.targets.push_back(pb);
+            P.targets.push_back(pe);
+            P.targets.push_back(s < nb ? 1 : 0);
+        }
+        P.fa_ptr[h + 1] = static_cast<int>(P.targets.size() / 4);
+        for (int t = P.level_ptr[h]; t < P.level_ptr[h + 1]; ++t) {
+            int k = P.level_nodes[t];
+            for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
+                P.scale.push_back(Lbase + p);
+                P.scale.push_back(k);
+            }
+        }
+        P.fb_ptr[h + 1] = static_cast<int>(P.scale.size() / 2);
+    }
+    if (P.n_pairs > INT32_MAX / 2) {
+        set_error("factorisation schedule too large for 32-bit pair indices");
+        return false;
+    }
+
+    // ---- forward-solve row lists ----
+    P.rptr.assign(nb + 1, 0);
+    for (int p = 0; p < nnzl; ++p) P.rptr[P.lidx[p] + 1]++;
+    for (int k = 0; k < nb; ++k) P.rptr[k + 1] += P.rptr[k];
+    P.rlist.assign(static_cast<size_t>(nnzl) * 2, 0);
+    {
+        std::vector<int> fp(P.rptr.begin(), P.rptr.end() - 1);
+        for (int m = 0; m < nb; ++m)
+            for (int p = P.lptr[m]; p < P.lptr[m + 1]; ++p) {
+                int k = P.lidx[p];
+                int q = fp[k]++;
+                P.rlist[2 * q] = Lbase + p;
+                P.rlist[2 * q + 1] = m;
+            }
+    }
+
+    // ---- reference variable / equation order ----
+    std::vector<int> ang(n_bus, -1), mag(n_bus, -1), peq(n_bus, -1), qeq(n_bus, -1);
+    {
+        int c = 0;
+        for (int i = 0; i < n_bus; ++i)
+            if (bus_type[i] != 2) ang[i] = c++;
+        for (int i = 0; i < n_bus; ++i)
+            if (bus_type[i] == 0) mag[i] = c++;
+        int r = 0;
+        for (int i = 0; i < n_bus; ++i) {
+            if (bus_type[i] == 2) continue;
+            peq[i] = r++;
+            if (bus_type[i] == 0) qeq[i] = r++;
+        }
+    }
+    P.var_of_comp.assign(2 * nb, -1);
+    P.eq_of_comp.assign(2 * nb, -1);
+    for (int k = 0; k < nb; ++k) {
+        int i = P.bus_of_node[k];
+        P.var_of_comp[2 * k] = ang[i];
+        P.var_of_comp[2 * k + 1] = mag[i];
+        P.eq_of_comp[2 * k] = peq[i];
+        P.eq_of_comp[2 * k + 1] = qeq[i];
+    }
+    return true;
+}
+
+}  // namespace gapk

@@ -1,0 +1,202 @@
+// Y-bus value assembly on the device and the gapk_ybus_* C ABI.
+//
+// One thread per (scenario, CSR slot).  An off-diagonal slot holds the stamp of the one
+// branch triplet that produced it; a diagonal slot sums its bus's shunt and branch-end stamps
+// sequentially in the reference's accumulation order (shunts in appliance order, then branch
+// ends in branch order), so the result is deterministic and, in reference mode, bit-identical
+// to src/admittance/cpu/cpu_admittance_matrix.cpp:88-145.  No atomics.
+//
+// All reference-mode arithmetic uses explicitly rounded intrinsics (__dmul_rn, __dadd_rn,
+// __ddiv_rn) so that no multiply-add is contracted into an FMA: the reference computes
+// r*r + x*x with two roundings.
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/gapk.h"
+#include "internal.h"
+
+namespace gapk {
+namespace {
+
+struct Stamps {
+    double2 ff, tt, ft, tf;
+};
+
+__device__ __forceinline__ Stamps branch_stamps(const double* __restrict__ br, int mode) {
+    const double r = br[0], x = br[1], g = br[2], b = br[3], k = br[4], th = br[5];
+    const double z2 = __dadd_rn(__dmul_rn(r, r), __dmul_rn(x, x));
+    double yr = 0.0, yi = 0.0;
+    if (z2 > 1e-12) {
+        yr = __ddiv_rn(r, z2);
+        yi = __ddiv_rn(-x, z2);
+    }
+    // end stamp y + g1 + j b1/2 (cpu_admittance_matrix.cpp:130-135)
+    const double er = __dadd_rn(__dadd_rn(yr, g), 0.0);
+    const double ei = __dadd_rn(__dadd_rn(yi, 0.0), __ddiv_rn(b, 2.0));
+    Stamps s;
+    if (mode == GAPK_YBUS_REFERENCE || (k == 1.0 && th == 0.0)) {
+        s.ff = make_double2(er, ei);
+        s.tt = s.ff;
+        s.ft = make_double2(-yr, -yi);
+        s.tf = s.ft;
+    } else {
+        // tap t = k e^{j th} on the from side: Y_ff = (y+ysh)/k^2, Y_ft = -y/conj(t),
+        // Y_tf = -y/t, Y_tt = y+ysh
+        double sn, cs;
+        sincos(th, &sn, &cs);
+        const double k2 = k * k;
+        s.ff = make_double2(er / k2, ei / k2);
+        s.tt = make_double2(er, ei);
+        // -y / conj(t) = -y * t / k^2 ;  -y / t = -y * conj(t) / k^2
+        const double tr = k * cs, ti = k * sn;
+        s.ft = make_double2(-(yr * tr - yi * ti) / k2, -(yr * ti + yi * tr) / k2);
+        s.tf = make_double2(-(yr * tr + yi * ti) / k2, -(yi * tr - yr * ti) / k2);
+    }
+    return s;
+}
+
+__global__ void k_ybus(int nnz, int n_scen, const int* __restrict__ slot_src,
+                       const int* __restrict__ diag_ptr, const int* __restrict__ diag_src,
+                       const double* __restrict__ br, long long br_stride,
+                       const double* __restrict__ sh, long long sh_stride, int mode,
+                       double scale, double2* __restrict__ out, long long out_stride) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long long)nnz * n_scen) return;
+    const int s = (int)(tid / nnz), p = (int)(tid % nnz);
+    const double* B = br + (size_t)s * br_stride;
+    const double* S = sh + (size_t)s * sh_stride;
+    const int src = slot_src[p];
+    double vr, vi;
+    if (src >= 0) {
+        const Stamps st = branch_stamps(B + (size_t)(src >> 1) * 6, mode);
+        const double2 v = (src & 1) ? st.tf : st.ft;
+        vr = v.x;
+        vi = v.y;
+    } else {
+        const int i = -src - 1;
+        vr = 0.0;
+        vi = 0.0;
+        for (int c = diag_ptr[i]; c < diag_ptr[i + 1]; ++c) {
+            const int d = diag_src[c];
+            if (d < 0) {
+                const double* q = S + (size_t)(-d - 1) * 2;
+                vr = __dadd_rn(vr, q[0]);
+                vi = __dadd_rn(vi, q[1]);
+            } else {
+                const Stamps st = branch_stamps(B + (size_t)(d >> 1) * 6, mode);
+                const double2 v = (d & 1) ? st.tt : st.ff;
+                vr = __dadd_rn(vr, v.x);
+                vi = __dadd_rn(vi, v.y);
+            }
+        }
+    }
+    if (scale != 1.0) {
+        vr = __dmul_rn(vr, scale);
+        vi = __dmul_rn(vi, scale);
+    }
+    out[(size_t)s * out_stride + p] = make_double2(vr, vi);
+}
+
+}  // namespace
+}  // namespace gapk
+
+using namespace gapk;
+
+struct gapk_ybus_s {
+    YbusPatternHost h;
+    int device = -1;
+    void* d_slot_src = nullptr;
+    void* d_diag_ptr = nullptr;
+    void* d_diag_src = nullptr;
+    ~gapk_ybus_s() {
+        if (d_slot_src) cudaFree(d_slot_src);
+        if (d_diag_ptr) cudaFree(d_diag_ptr);
+        if (d_diag_src) cudaFree(d_diag_src);
+    }
+    int upload() {
+        if (d_slot_src) return GAPK_OK;
+        auto up = [](void*& d, std::vector<int> const& v) -> cudaError_t {
+            size_t bytes = (v.empty() ? 1 : v.size()) * sizeof(int);
+            cudaError_t e = cudaMalloc(&d, bytes);
+            if (e != cudaSuccess) return e;
+            if (!v.empty()) e = cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice);
+            return e;
+        };
+        cudaError_t e = up(d_slot_src, h.slot_src);
+        if (e == cudaSuccess) e = up(d_diag_ptr, h.diag_ptr);
+        if (e == cudaSuccess) e = up(d_diag_src, h.diag_src);
+        if (e != cudaSuccess) {
+            set_error(std::string("ybus upload: ") + cudaGetErrorString(e));
+            return e == cudaErrorMemoryAllocation ? GAPK_ENOMEM : GAPK_ECUDA;
+        }
+        cudaGetDevice(&device);
+        return GAPK_OK;
+    }
+};
+
+extern "C" {
+
+int gapk_ybus_create(int n_bus, int n_branch, const int* h_from_idx, const int* h_to_idx,
+                     const int* h_in_service, int n_shunt, const int* h_shunt_bus,
+                     gapk_ybus* out) {
+    if (!out || n_bus < 0 || n_branch < 0 || n_shunt < 0 ||
+        (n_branch && (!h_from_idx || !h_to_idx || !h_in_service)) || (n_shunt && !h_shunt_bus)) {
+        set_error("gapk_ybus_create: bad arguments");
+        return GAPK_EINVAL;
+    }
+    auto y = std::make_unique<gapk_ybus_s>();
+    build_ybus_pattern(n_bus, n_branch, h_from_idx, h_to_idx, h_in_service, n_shunt,
+                       h_shunt_bus, y->h);
+    *out = y.release();
+    return GAPK_OK;
+}
+
+int gapk_ybus_destroy(gapk_ybus y) {
+    delete y;
+    return GAPK_OK;
+}
+
+int gapk_ybus_nnz(gapk_ybus y) { return y ? y->h.nnz : GAPK_EINVAL; }
+
+int gapk_ybus_pattern(gapk_ybus y, int* h_row_ptr, int* h_col_idx) {
+    if (!y || !h_row_ptr || (y->h.nnz && !h_col_idx)) {
+        set_error("gapk_ybus_pattern: bad arguments");
+        return GAPK_EINVAL;
+    }
+    std::copy(y->h.row_ptr.begin(), y->h.row_ptr.end(), h_row_ptr);
+    std::copy(y->h.col_idx.begin(), y->h.col_idx.end(), h_col_idx);
+    return GAPK_OK;
+}
+
+int gapk_ybus_assemble(gapk_ybus y, int n_scen, const double* d_branch, int64_t branch_stride,
+                       const double* d_shunt, int64_t shunt_stride, int mode, double scale,
+                       double* d_values, int64_t values_stride, void* stream) {
+    if (!y || n_scen <= 0 || !d_values || (y->h.n_branch && !d_branch) ||
+        (y->h.n_shunt && !d_shunt) || (mode != GAPK_YBUS_REFERENCE && mode != GAPK_YBUS_TAPS) ||
+        branch_stride < 0 || shunt_stride < 0 || (n_scen > 1 && values_stride < y->h.nnz)) {
+        set_error("gapk_ybus_assemble: bad arguments");
+        return GAPK_EINVAL;
+    }
+    int rc = y->upload();
+    if (rc) return rc;
+    const long long total = (long long)y->h.nnz * n_scen;
+    if (total == 0) return GAPK_OK;
+    const int thr = 256;
+    const unsigned blocks = static_cast<unsigned>((total + thr - 1) / thr);
+    k_ybus<<<blocks, thr, 0, static_cast<cudaStream_t>(stream)>>>(
+        y->h.nnz, n_scen, static_cast<const int*>(y->d_slot_src),
+        static_cast<const int*>(y->d_diag_ptr), static_cast<const int*>(y->d_diag_src),
+        d_branch, branch_stride, d_shunt, shunt_stride, mode, scale,
+        reinterpret_cast<double2*>(d_values), values_stride);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("k_ybus launch: ") + cudaGetErrorString(e));
+        return GAPK_ECUDA;
+    }
+    return GAPK_OK;
+}
+
+}  // extern "C"

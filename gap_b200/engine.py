@@ -1,0 +1,261 @@
+"""Python host layer over libgapk.so: Y-bus builder, Newton-Raphson plans and batches.
+
+Device memory and streams come from PyTorch (tensors on cuda, torch's current stream); all
+compute runs in the library's sm_100a kernels.  There is no CPU fallback: on a machine
+without the library or without a GPU these classes raise.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .network import PQ, PV, SLACK, Network
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _stream_ptr(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _dptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def require_cuda():
+    torch = _torch()
+    if not torch.cuda.is_available():
+        raise RuntimeError("gap_b200 needs a CUDA device (no CPU fallback on the product path)")
+    N.lib()
+
+
+# ----------------------------------------------------------------------------------------
+# Y-bus
+# ----------------------------------------------------------------------------------------
+
+
+class YbusPlan:
+    """CSR pattern of one topology (host, built once) + device value assembly.
+
+    Replaces IAdmittanceMatrix::build_admittance_matrix
+    (include/gap/admittance/admittance_interface.h:21-22): the pattern equals the reference's
+    stable-sorted triplet order (src/admittance/cpu/cpu_admittance_matrix.cpp:100-186)."""
+
+    def __init__(self, n_bus, from_idx, to_idx, in_service, shunt_bus=()):
+        L = N.lib()
+        self.n_bus = int(n_bus)
+        f = N.i32(from_idx)
+        t = N.i32(to_idx)
+        s = N.i32(in_service)
+        sb = N.i32(shunt_bus)
+        self.n_branch = int(f.size)
+        self.n_shunt = int(sb.size)
+        h = C.c_void_p()
+        N.check(L.gapk_ybus_create(C.c_int(self.n_bus), C.c_int(self.n_branch), N.iptr(f),
+                                   N.iptr(t), N.iptr(s), C.c_int(self.n_shunt), N.iptr(sb),
+                                   C.byref(h)))
+        self._h = h
+        self.nnz = int(L.gapk_ybus_nnz(h))
+        self.row_ptr = np.zeros(self.n_bus + 1, np.int32)
+        self.col_idx = np.zeros(self.nnz, np.int32)
+        N.check(L.gapk_ybus_pattern(h, N.iptr(self.row_ptr), N.iptr(self.col_idx)))
+
+    @staticmethod
+    def from_network(net: Network) -> "YbusPlan":
+        f, t, valid = net.branch_index()
+        sb, _, _ = net.shunt_index()
+        return YbusPlan(net.n_bus, np.where(valid, f, 0), np.where(valid, t, 0),
+                        valid.astype(np.int32), sb)
+
+    def assemble(self, branch, shunt=None, mode=N.YBUS_REFERENCE, scale=1.0, stream=None):
+        """branch: cuda float64 [m, 6] or [S, m, 6] = (r1, x1, g1, b1, k, theta);
+        shunt: [n_shunt, 2] or [S, n_shunt, 2] = (g1, b1).  Returns complex128 [S, nnz]
+        (S = 1 for unbatched input)."""
+        torch = _torch()
+        br = branch.contiguous()
+        S = br.shape[0] if br.dim() == 3 else 1
+        bst = self.n_branch * 6 if br.dim() == 3 else 0
+        if shunt is None:
+            shunt = torch.zeros((max(self.n_shunt, 1), 2), dtype=torch.float64, device=br.device)
+        sh = shunt.contiguous()
+        sst = self.n_shunt * 2 if sh.dim() == 3 else 0
+        out = torch.empty((S, self.nnz), dtype=torch.complex128, device=br.device)
+        N.check(N.lib().gapk_ybus_assemble(self._h, S, _dptr(br), bst, _dptr(sh), sst, mode,
+                                           float(scale), _dptr(out), self.nnz,
+                                           _stream_ptr(stream)))
+        return out
+
+    def __del__(self):
+        try:
+            if self._h:
+                N.lib().gapk_ybus_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+def branch_params(net: Network) -> np.ndarray:
+    """[m, 6] float64 = (r1, x1, g1, b1, k, theta) per branch, in the network's units."""
+    return np.stack([net.r1, net.x1, net.g1, net.b1, net.k, net.theta], axis=1).astype(np.float64)
+
+
+def shunt_params(net: Network) -> np.ndarray:
+    sb, g, b = net.shunt_index()
+    if len(sb) == 0:
+        return np.zeros((1, 2))
+    return np.stack([np.asarray(g, np.float64), np.asarray(b, np.float64)], axis=1)
+
+
+# ----------------------------------------------------------------------------------------
+# Newton-Raphson
+# ----------------------------------------------------------------------------------------
+
+_EXPORT = dict(bus_of_node=0, node_pq=1, lptr=2, lidx=3, level_ptr=4, level_nodes=5,
+               slot_info=6, slot_src_ptr=7, slot_src=8, fa_ptr=9, targets=10, pairs=11,
+               fb_ptr=12, scale=13, rptr=14, rlist=15, var_of_comp=16, eq_of_comp=17,
+               slot_a=18, arow_ptr=19, arow=20)
+
+
+class NRPlan:
+    """Symbolic analysis of one (Y pattern, bus types) pair; shared by every batch and every
+    scenario with that pattern.  Host-only until a batch uploads it."""
+
+    def __init__(self, row_ptr, col_idx, bus_type, jacobian="reference", ordering="mindeg"):
+        L = N.lib()
+        rp = N.i32(row_ptr)
+        ci = N.i32(col_idx)
+        bt = N.i32(bus_type)
+        opt = N.PlanOptions(N.JAC_REFERENCE if jacobian == "reference" else N.JAC_EXACT,
+                            N.ORDER_MINDEG if ordering == "mindeg" else N.ORDER_NATURAL)
+        h = C.c_void_p()
+        N.check(L.gapk_nr_plan_create(C.c_int(len(rp) - 1), C.c_int(len(ci)), N.iptr(rp),
+                                      N.iptr(ci), N.iptr(bt), C.byref(opt), C.byref(h)))
+        self._h = h
+        self.row_ptr, self.col_idx, self.bus_type = rp, ci, bt
+        info = N.PlanInfo()
+        N.check(L.gapk_nr_plan_get_info(h, C.byref(info)))
+        self.info = info.as_dict()
+
+    def export(self, name):
+        L = N.lib()
+        w = _EXPORT[name]
+        n = L.gapk_nr_plan_export(self._h, w, None)
+        if n < 0:
+            N.check(int(n))
+        buf = np.zeros(max(int(n), 1), np.int32)
+        L.gapk_nr_plan_export(self._h, w, N.iptr(buf))
+        return buf[: int(n)]
+
+    def __del__(self):
+        try:
+            if self._h:
+                N.lib().gapk_nr_plan_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+@dataclass
+class NRResult:
+    v: "object"            # complex128 [S, n_bus] (torch, cuda)
+    iterations: "object"   # int32 [S]
+    status: "object"       # int32 [S]
+    final_mismatch: "object"  # float64 [S]
+
+    @property
+    def converged(self):
+        return self.status == N.SCEN_CONVERGED
+
+
+class NRBatch:
+    """Device state for n_scen scenarios sharing one NRPlan."""
+
+    def __init__(self, plan: NRPlan, n_scen: int, precision="fp64", y_shared=True, lanes=0,
+                 threads=0, use_graph=True):
+        require_cuda()
+        self.plan = plan
+        self.n_scen = int(n_scen)
+        self.precision = precision
+        self.y_shared = bool(y_shared)
+        opt = N.BatchOptions(N.PREC_FP64 if precision == "fp64" else N.PREC_FP32,
+                             1 if y_shared else 0, int(lanes), int(threads),
+                             1 if use_graph else 0)
+        h = C.c_void_p()
+        N.check(N.lib().gapk_nr_batch_create(plan._h, C.c_int(self.n_scen), C.byref(opt),
+                                             C.byref(h)))
+        self._h = h
+
+    @property
+    def device_bytes(self):
+        return int(N.lib().gapk_nr_batch_device_bytes(self._h))
+
+    def _inputs(self, y, s_spec, v_init, u_pu, tol, max_iter, policy, refine):
+        pol = N.POLICY_REFERENCE if policy == "reference" else N.POLICY_NEWTON
+        return N.Inputs(_dptr(y), _dptr(s_spec), _dptr(v_init), _dptr(u_pu), float(tol),
+                        int(max_iter), pol, int(refine))
+
+    def solve(self, y, s_spec, v_init=None, u_pu=None, tol=1e-8, max_iter=20,
+              policy="reference", refine=0, out=None, stream=None) -> NRResult:
+        """y: complex128 per-unit Y values, [nnz] (y_shared) or [S, nnz]; s_spec: complex128
+        [S, n_bus]; v_init: complex128 [S, n_bus] or None (flat start); u_pu: float64
+        [n_bus] flat-start |V| of SLACK/PV buses."""
+        torch = _torch()
+        n = self.plan.info["n_bus"]
+        dev = s_spec.device
+        if out is None:
+            out = NRResult(torch.empty((self.n_scen, n), dtype=torch.complex128, device=dev),
+                           torch.empty(self.n_scen, dtype=torch.int32, device=dev),
+                           torch.empty(self.n_scen, dtype=torch.int32, device=dev),
+                           torch.empty(self.n_scen, dtype=torch.float64, device=dev))
+        inp = self._inputs(y, s_spec, v_init, u_pu, tol, max_iter, policy, refine)
+        o = N.Outputs(_dptr(out.v), _dptr(out.iterations), _dptr(out.status),
+                      _dptr(out.final_mismatch))
+        N.check(N.lib().gapk_nr_solve(self._h, C.byref(inp), C.byref(o), _stream_ptr(stream)))
+        return out
+
+    # stage access (tests, profiling)
+    def stage_load(self, y, s_spec, v_init=None, u_pu=None, refine=0, stream=None):
+        inp = self._inputs(y, s_spec, v_init, u_pu, 0.0, 1, "newton", refine)
+        N.check(N.lib().gapk_nr_stage_load(self._h, C.byref(inp), _stream_ptr(stream)))
+
+    def stage(self, name, stream=None):
+        fn = {"mismatch": "gapk_nr_stage_mismatch", "jacobian": "gapk_nr_stage_jacobian",
+              "factor": "gapk_nr_stage_factor", "solve": "gapk_nr_stage_solve"}[name]
+        N.check(getattr(N.lib(), fn)(self._h, _stream_ptr(stream)))
+
+    def correction(self, stream=None):
+        torch = _torch()
+        nv = self.plan.info["n_vars"]
+        out = torch.zeros((self.n_scen, nv), dtype=torch.float64, device="cuda")
+        N.check(N.lib().gapk_nr_stage_get_correction(self._h, _dptr(out), _stream_ptr(stream)))
+        return out
+
+    def mismatch(self, stream=None):
+        torch = _torch()
+        nv = self.plan.info["n_vars"]
+        out = torch.zeros((self.n_scen, nv), dtype=torch.float64, device="cuda")
+        N.check(N.lib().gapk_nr_stage_get_mismatch(self._h, _dptr(out), _stream_ptr(stream)))
+        return out
+
+    def loop_count(self, stream=None):
+        v = C.c_int(0)
+        N.check(N.lib().gapk_nr_last_loop_count(self._h, _stream_ptr(stream), C.byref(v)))
+        return v.value
+
+    def __del__(self):
+        try:
+            if self._h:
+                N.lib().gapk_nr_batch_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass

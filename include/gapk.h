@@ -1,0 +1,211 @@
+/*
+ * gapk.h -- C ABI of the B200 Newton-Raphson power-flow engine (libgapk.so).
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes.  Device pointers are
+ * marked d_*, host pointers h_*.  Complex numbers are two interleaved doubles (re, im).
+ * Every call that launches GPU work takes a cudaStream_t (passed as void*; NULL = the legacy
+ * default stream) and does not synchronise unless it says so.
+ *
+ * Which reference interface each group replaces (paths inside the reference project):
+ *
+ *   gapk_ybus_*      gap::admittance::IAdmittanceMatrix::build_admittance_matrix /
+ *                    update_admittance_matrix (include/gap/admittance/admittance_interface.h:21-31),
+ *                    GPU implementation src/admittance/gpu/gpu_admittance_matrix.cu:243-410,
+ *                    CPU semantics src/admittance/cpu/cpu_admittance_matrix.cpp:44-301.
+ *   gapk_nr_*        gap::solver::IPowerFlowSolver::solve_power_flow
+ *                    (include/gap/solver/powerflow_interface.h:59-61), GPU implementation
+ *                    src/solver/powerflow/gpu/gpu_newton_raphson.cu:392-570 and its kernels
+ *                    src/solver/powerflow/gpu/gpu_powerflow_kernels.cu:16-538, CPU semantics
+ *                    src/solver/powerflow/cpu/cpu_newton_raphson.cpp:33-727.
+ *   gapk_splu_*      gap::solver::ILUSolver::factorize / solve / update_factorization
+ *                    (include/gap/solver/lu_solver_interface.h:21-35), GPU implementation
+ *                    src/solver/lu/gpu/gpu_cudss_solver.cu:167-479.
+ *   gapk_nr_adjoint  no counterpart in the reference (gradients through the converged state).
+ *
+ * The C++ plugin libraries libgap_{admittance,lu,powerflow}_gpu.so export the reference's
+ * factory symbols (create_gpu_* / destroy_gpu_*) and call these functions.
+ */
+#ifndef GAPK_H
+#define GAPK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------- */
+#define GAPK_OK 0
+#define GAPK_EINVAL (-1)   /* bad argument (message in gapk_last_error)                   */
+#define GAPK_ECUDA (-2)    /* CUDA runtime error                                          */
+#define GAPK_ENOMEM (-3)   /* device allocation failed                                    */
+#define GAPK_ESTATE (-4)   /* call out of order (e.g. solve before factorize)             */
+#define GAPK_ESINGULAR (-5) /* zero / non-finite pivot                                    */
+#define GAPK_ERANGE (-6)   /* size beyond a documented maximum                            */
+
+/* per-scenario solve status */
+#define GAPK_SCEN_CONVERGED 0
+#define GAPK_SCEN_MAXITER 1
+#define GAPK_SCEN_SINGULAR 2
+#define GAPK_SCEN_NONFINITE 3
+
+/* bus types, as gap::BusType (include/gap/core/types.h:30-34) */
+#define GAPK_BUS_PQ 0
+#define GAPK_BUS_PV 1
+#define GAPK_BUS_SLACK 2
+
+/* Message for the last failing call on this thread (never NULL). */
+const char* gapk_last_error(void);
+/* ABI version: major*10000 + minor*100 + patch. */
+int gapk_version(void);
+/* Number of CUDA devices visible (0 when none); never fails. */
+int gapk_device_count(void);
+
+/* ==== Y-bus ============================================================================
+ * The CSR pattern is built on the host once per topology, bit-identical to the reference's
+ * stable-sorted triplet order (duplicates from parallel branches kept, diagonal of every bus
+ * present).  Values are assembled on the device as a deterministic segmented reduction: each
+ * diagonal sums its shunt and branch-end stamps in the reference's order, without atomics.
+ */
+typedef struct gapk_ybus_s* gapk_ybus;
+
+/* from_idx / to_idx are bus positions (0..n_bus-1); in_service != 0 marks branches that enter
+ * the matrix (the caller resolves IDs and drops invalid branches, as the reference does).
+ * shunt_bus lists the bus position of every shunt in appliance order. */
+int gapk_ybus_create(int n_bus, int n_branch, const int* h_from_idx, const int* h_to_idx,
+                     const int* h_in_service, int n_shunt, const int* h_shunt_bus,
+                     gapk_ybus* out);
+int gapk_ybus_destroy(gapk_ybus y);
+int gapk_ybus_nnz(gapk_ybus y);
+/* Copies the pattern out: h_row_ptr[n_bus+1], h_col_idx[nnz]. */
+int gapk_ybus_pattern(gapk_ybus y, int* h_row_ptr, int* h_col_idx);
+
+#define GAPK_YBUS_REFERENCE 0 /* ignore tap k and shift theta, as the reference builder   */
+#define GAPK_YBUS_TAPS 1      /* pi model with tap k*exp(j theta) on the from side        */
+
+/* Assemble values for n_scen scenarios.
+ *   d_branch : doubles [n_scen][n_branch][6] = (r1, x1, g1, b1, k, theta) per branch,
+ *              scenario stride branch_stride doubles (0 = shared by all scenarios)
+ *   d_shunt  : doubles [n_scen][n_shunt][2] = (g1, b1), stride shunt_stride (0 = shared)
+ *   d_values : complex [n_scen][nnz], stride values_stride complex entries
+ *   scale    : every value is multiplied by scale (1.0 = Siemens; Z_base = per unit)
+ */
+int gapk_ybus_assemble(gapk_ybus y, int n_scen, const double* d_branch, int64_t branch_stride,
+                       const double* d_shunt, int64_t shunt_stride, int mode, double scale,
+                       double* d_values, int64_t values_stride, void* stream);
+
+/* ==== Newton-Raphson engine ===========================================================
+ * A plan holds everything that depends only on the Y pattern and the bus types: the
+ * 2x2-block Jacobian pattern, a minimum-degree ordering, the symbolic block-LU
+ * factorisation, its level schedule and the Y->Jacobian scatter map.  Plans are built on the
+ * host and uploaded to the current device on first use.  A batch holds the device state of
+ * n_scen scenarios that share one plan.
+ */
+typedef struct gapk_nr_plan_s* gapk_nr_plan;
+typedef struct gapk_nr_batch_s* gapk_nr_batch;
+
+#define GAPK_JAC_REFERENCE 0 /* duplicate Y entries: last one wins (reference dense G/B)  */
+#define GAPK_JAC_EXACT 1     /* duplicate Y entries summed (true derivative)              */
+
+#define GAPK_ORDER_MINDEG 0  /* minimum degree on the bus graph                            */
+#define GAPK_ORDER_NATURAL 1 /* bus order                                                  */
+
+typedef struct {
+    int jacobian_mode; /* GAPK_JAC_*                                                       */
+    int ordering;      /* GAPK_ORDER_*                                                     */
+} gapk_nr_plan_options;
+
+typedef struct {
+    int n_bus, n_block;   /* buses; block unknowns (non-slack buses)                       */
+    int n_pq, n_pv, n_slack;
+    int n_vars;           /* reference Newton unknowns: (n_bus - n_slack) + n_pq            */
+    int nnz_y;
+    int nnz_l_blocks;     /* strictly-lower blocks of L (= of U^T)                          */
+    int n_slots;          /* n_block + 2 * nnz_l_blocks                                     */
+    int n_a_blocks;       /* blocks of the Jacobian pattern itself                          */
+    int n_levels;         /* elimination-tree height + 1                                    */
+    int64_t n_pairs;      /* block multiply-adds of one numeric factorisation               */
+    int64_t n_rows_pairs; /* block multiply-adds of one forward solve                       */
+    int max_level_width;
+} gapk_nr_plan_info;
+
+int gapk_nr_plan_create(int n_bus, int nnz_y, const int* h_y_row_ptr, const int* h_y_col_idx,
+                        const int* h_bus_type, const gapk_nr_plan_options* opt,
+                        gapk_nr_plan* out);
+int gapk_nr_plan_destroy(gapk_nr_plan p);
+int gapk_nr_plan_get_info(gapk_nr_plan p, gapk_nr_plan_info* info);
+
+/* Export host-side schedule arrays (for inspection and CPU-side checking).  `what` selects:
+ *   0 bus_of_node[n_block]   1 node_pq[n_block]      2 lptr[n_block+1]   3 lidx[nnz_l]
+ *   4 level_ptr[n_levels+1]  5 level_nodes[n_block]  6 slot_info[n_slots*4]
+ *   7 slot_src_ptr[n_slots+1] 8 slot_src[...]        9 fa_ptr[n_levels+1]
+ *  10 targets[n_targets*4]  11 pairs[n_pairs*2]     12 fb_ptr[n_levels+1] 13 scale[n_b*2]
+ *  14 rptr[n_block+1]       15 rlist[...*2]
+ * Returns the number of ints written (or needed when h_buf is NULL). */
+int64_t gapk_nr_plan_export(gapk_nr_plan p, int what, int* h_buf);
+
+#define GAPK_PREC_FP64 0  /* factor and triangular solves in FP64                          */
+#define GAPK_PREC_FP32 1  /* factor and triangular solves in FP32 (mismatch, update and
+                             convergence stay FP64)                                        */
+
+typedef struct {
+    int precision;      /* GAPK_PREC_*                                                     */
+    int y_shared;       /* 1: one Y for all scenarios; 0: one Y per scenario               */
+    int lanes;          /* scenarios interleaved per thread group: 1, 2, 4 or 8 (0 = auto) */
+    int threads;        /* threads per CTA of the factor / solve kernels (0 = auto)        */
+    int use_graph;      /* 1: NR loop as a CUDA graph with a device-side while node        */
+} gapk_nr_batch_options;
+
+int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options* opt,
+                         gapk_nr_batch* out);
+int gapk_nr_batch_destroy(gapk_nr_batch b);
+/* Device bytes held by the batch. */
+int64_t gapk_nr_batch_device_bytes(gapk_nr_batch b);
+
+#define GAPK_POLICY_REFERENCE 0 /* damping 0.9, |dtheta|<=0.15, |d|V||<=0.08, |V| in [0.5,1.5]
+                                   (cpu_newton_raphson.cpp:438-504)                         */
+#define GAPK_POLICY_NEWTON 1    /* full Newton step                                         */
+
+typedef struct {
+    const double* d_y;      /* complex Y (per unit): [nnz] if y_shared else [n_scen][nnz] */
+    const double* d_s_spec; /* complex specified injections (per unit) [n_scen][n_bus]    */
+    const double* d_v_init; /* complex start voltages [n_scen][n_bus], or NULL = flat start */
+    const double* d_u_pu;   /* flat-start |V| of SLACK/PV buses [n_bus] (NULL = 1.0)        */
+    double tolerance;       /* on max |mismatch| in per unit                                */
+    int max_iterations;
+    int policy;             /* GAPK_POLICY_*                                                */
+    int refine;             /* extra iterative-refinement steps on each Newton correction  */
+} gapk_nr_inputs;
+
+typedef struct {
+    double* d_v;              /* complex [n_scen][n_bus] (may be NULL)                    */
+    int* d_iterations;        /* [n_scen] (may be NULL)                                   */
+    int* d_status;            /* [n_scen] GAPK_SCEN_* (may be NULL)                       */
+    double* d_final_mismatch; /* [n_scen] (may be NULL)                                   */
+} gapk_nr_outputs;
+
+/* Runs the whole Newton-Raphson loop on the device.  Asynchronous on `stream`. */
+int gapk_nr_solve(gapk_nr_batch b, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
+                  void* stream);
+
+/* Device counters of the last solve, copied to the host (synchronises the stream):
+ * h_counters[0] = Newton iterations run by the device loop (max over scenarios). */
+int gapk_nr_last_loop_count(gapk_nr_batch b, void* stream, int* h_loops);
+
+/* ---- building blocks, one launch each (used for timing and for tests) ----------------- */
+/* Copy inputs into the batch and flat-start; afterwards the kernels below may be run. */
+int gapk_nr_stage_load(gapk_nr_batch b, const gapk_nr_inputs* in, void* stream);
+int gapk_nr_stage_mismatch(gapk_nr_batch b, void* stream);
+int gapk_nr_stage_jacobian(gapk_nr_batch b, void* stream);
+int gapk_nr_stage_factor(gapk_nr_batch b, void* stream);
+int gapk_nr_stage_solve(gapk_nr_batch b, void* stream);
+/* Newton correction of the last stage_solve, [n_scen][n_vars] doubles in the reference's
+ * variable order (theta of non-slack buses, then |V| of PQ buses). */
+int gapk_nr_stage_get_correction(gapk_nr_batch b, double* d_dx, void* stream);
+/* Mismatch of the last stage_mismatch, [n_scen][n_vars] in the reference's equation order. */
+int gapk_nr_stage_get_mismatch(gapk_nr_batch b, double* d_f, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GAPK_H */

@@ -1,0 +1,228 @@
+"""GPU parity: the sm_100a path (through libgapk.so's C ABI) against the oracle and the
+reference's golden outputs.
+
+Tolerances (from the engine's parity contract): CSR pattern and reference-mode Y-bus values
+bit-exact; tap-mode Y-bus 1e-14 relative; converged |V| and angle within 1e-8 pu / rad of the
+reference CPU solver and iteration count within +-1; mismatch 1e-9 relative; FP64 Newton
+correction 1e-10 relative."""
+
+import numpy as np
+import pytest
+
+from helpers import fixture_names, load, network_of, parity_fixtures
+from oracle import restate
+
+pytestmark = pytest.mark.gpu
+
+FIX = [n for n in parity_fixtures() if n != "kat_update"]
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+@pytest.mark.parametrize("name", FIX)
+def test_ybus_device_values_bit_exact(name):
+    from gap_b200.api import AdmittanceMatrix
+
+    net, d = network_of(name)
+    rp, ci, va = AdmittanceMatrix().build_admittance_matrix(net)
+    assert np.array_equal(rp, d["y_row_ptr"]) and np.array_equal(ci, d["y_col_idx"])
+    assert np.array_equal(va, d["y_values"])
+
+
+def test_ybus_taps_mode_matches_pi_model():
+    from gap_b200 import synth
+    from gap_b200.api import AdmittanceMatrix
+
+    net = synth.transmission_grid(2, n=600)
+    rp, ci, va = AdmittanceMatrix(taps=True).build_admittance_matrix(net)
+    rp2, ci2, vb = restate.ybus_pi(net)
+    assert np.array_equal(rp, rp2) and np.array_equal(ci, ci2)
+    scale = np.max(np.abs(vb))
+    assert np.max(np.abs(va - vb)) <= 1e-14 * scale
+
+
+def test_ybus_batched_scenarios():
+    """Per-scenario branch parameters (here: outages as zero admittance rows) in one launch."""
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import YbusPlan, branch_params, shunt_params
+
+    net = synth.transmission_grid(4, n=300)
+    yp = YbusPlan.from_network(net)
+    br = np.repeat(branch_params(net)[None], 5, axis=0)
+    rng = np.random.default_rng(0)
+    br[:, :, 0] *= rng.uniform(0.9, 1.1, size=br.shape[:2])
+    out = yp.assemble(torch.as_tensor(br, device="cuda"),
+                      torch.as_tensor(shunt_params(net), device="cuda"), mode=1).cpu().numpy()
+    for s in range(5):
+        n2 = synth.transmission_grid(4, n=300)
+        n2.r1 = br[s, :, 0].copy()
+        _, _, ref = restate.ybus_pi(n2)
+        assert np.max(np.abs(out[s] - ref)) <= 1e-14 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("name", fixture_names("pgm_"))
+def test_solve_simple_power_flow_pgm(name):
+    """The reference's pytest contract (test_pgm_validation.py:213-252) plus parity with the
+    reference CPU solver on the same lists."""
+    from gap_b200.api import solve_simple_power_flow
+
+    d = load(name)
+    out = solve_simple_power_flow(d["bus_data"].tolist(), d["branch_data"].tolist(),
+                                  tolerance=1e-8, max_iterations=20, verbose=False,
+                                  base_power=float(d["base_power"]), backend="gpu")
+    meta = out[-1]
+    rows = np.array(out[:-1])
+    assert bool(meta[0]) and bool(d["ref_converged"])
+    assert abs(int(meta[1]) - int(d["ref_iterations"])) <= 1
+    assert np.max(np.abs(rows[:, 2] - d["pgm_u_pu"])) < 5e-6
+    assert np.max(np.abs(rows[:, 2] - np.abs(d["ref_v"]))) < 1e-8
+    assert np.max(np.abs(rows[:, 3] - np.angle(d["ref_v"]))) < 1e-8
+
+
+@pytest.mark.parametrize("name", fixture_names("c0_") + fixture_names("kat_"))
+def test_nr_fp64_matches_reference(name):
+    if name == "kat_update":
+        pytest.skip("no solve")
+    from gap_b200.api import NewtonRaphson, PowerFlowConfig
+
+    net, d = network_of(name)
+    cfg = PowerFlowConfig(tolerance=1e-8, max_iterations=20, base_power=float(d["base_power"]))
+    Y = (d["y_row_ptr"], d["y_col_idx"], d["y_values"])
+    r = NewtonRaphson().solve_power_flow(net, Y, cfg)
+    assert r.converged == bool(d["ref_converged"])
+    assert abs(r.iterations - int(d["ref_iterations"])) <= 1
+    if r.converged:
+        assert np.max(np.abs(np.abs(r.bus_voltages) - np.abs(d["ref_v"]))) < 1e-8
+        assert np.max(np.abs(np.angle(r.bus_voltages) - np.angle(d["ref_v"]))) < 1e-8
+    else:
+        # singular Jacobian (isolated bus): V stays where the reference leaves it
+        np.testing.assert_allclose(r.bus_voltages, d["ref_v"], atol=1e-12)
+        assert r.final_mismatch == pytest.approx(float(d["ref_final_mismatch"]), rel=1e-9)
+
+
+@pytest.mark.parametrize("name", [n for n in fixture_names("kat_") if n != "kat_update"])
+def test_mismatch_matches_reference(name):
+    from gap_b200.api import NewtonRaphson
+
+    net, d = network_of(name)
+    nr = NewtonRaphson()
+    for k in ("0", "1"):
+        f = nr.calculate_mismatches(net, d["mm_v" + k])
+        np.testing.assert_allclose(f, d["mm_f" + k], rtol=1e-9, atol=1e-6)
+
+
+@pytest.mark.parametrize("precision,lanes", [("fp64", 1), ("fp64", 4), ("fp32", 8)])
+def test_newton_correction_matches_sparse_solve(precision, lanes):
+    """One Jacobian build + factor + solve on the device vs scipy on the oracle Jacobian."""
+    torch = _torch()
+    import scipy.sparse.linalg as spla
+
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.transmission_grid(7, n=1000)
+    base = 1e8
+    zb = net.u_rated[0] ** 2 / base
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
+    S = 6
+    rng = np.random.default_rng(3)
+    v = np.stack([restate.flat_start(net) * np.exp(1j * rng.normal(0, 0.03, net.n_bus))
+                  for _ in range(S)])
+    s_spec = np.repeat(net.specified_power(base)[None], S, axis=0)
+    b = NRBatch(plan, S, precision=precision, lanes=lanes)
+    b.stage_load(y, torch.as_tensor(s_spec, device="cuda"),
+                 v_init=torch.as_tensor(v, device="cuda"), refine=1 if precision == "fp32" else 0)
+    for st in ("mismatch", "jacobian", "factor", "solve"):
+        b.stage(st)
+    dx = b.correction().cpu().numpy()
+    f = b.mismatch().cpu().numpy()
+    ypu = y.cpu().numpy()
+    for s in range(S):
+        sc = restate.power_injections(yp.row_ptr, yp.col_idx, ypu, v[s])
+        fr = restate.mismatch(net.bus_type, sc, s_spec[s])
+        np.testing.assert_allclose(f[s], fr, rtol=1e-9, atol=1e-11)
+        J = restate.jacobian(yp.row_ptr, yp.col_idx, ypu, v[s], net.bus_type, mode="exact",
+                             drop=False)
+        xr = spla.spsolve(J.tocsc(), -fr)
+        tol = 1e-10 if precision == "fp64" else 1e-6
+        assert np.max(np.abs(dx[s] - xr)) <= tol * np.max(np.abs(xr))
+
+
+@pytest.mark.parametrize("precision,refine", [("fp64", 0), ("fp32", 1)])
+def test_batched_scenarios_match_oracle(precision, refine):
+    """Load scenarios of a transmission grid (taps, PV, shunts) in one batch, Newton policy,
+    against the FP64 oracle solved to the same tolerance."""
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.transmission_grid(1, n=2000)
+    base = 1e8
+    zb = net.u_rated[0] ** 2 / base
+    S = 19  # not a multiple of the lane count: exercises padding lanes
+    s_spec = synth.load_scenarios(net, S, sigma=0.1, seed=5, base_power=base)
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
+    b = NRBatch(plan, S, precision=precision, lanes=8)
+    r = b.solve(y, torch.as_tensor(s_spec, device="cuda"),
+                u_pu=torch.as_tensor(net.u_pu, device="cuda"), tol=1e-10, max_iter=30,
+                policy="newton", refine=refine)
+    torch.cuda.synchronize()
+    st = r.status.cpu().numpy()
+    assert (st == 0).all(), st
+    V = r.v.cpu().numpy()
+    Y = restate.ybus_pi(net)
+    for s in (0, 7, 8, 18):
+        o = restate.nr_solve(net, Y=Y, tol=1e-12, max_iter=30, base_power=base,
+                             policy="newton", jac="exact", s_spec=s_spec[s])
+        assert o["converged"]
+        assert np.max(np.abs(np.abs(V[s]) - np.abs(o["v"]))) < 1e-8
+        assert np.max(np.abs(np.angle(V[s]) - np.angle(o["v"]))) < 1e-8
+
+
+def test_graph_and_host_loop_agree():
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.feeder_grid(3)
+    zb = net.u_rated[0] ** 2 / 1e6
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type)
+    s = torch.as_tensor(net.specified_power(1e6)[None], device="cuda")
+    outs = []
+    for g in (True, False):
+        b = NRBatch(plan, 1, lanes=1, use_graph=g)
+        r = b.solve(y, s, tol=1e-8, max_iter=20)
+        torch.cuda.synchronize()
+        outs.append((r.v.cpu().numpy(), int(r.iterations[0]), b.loop_count()))
+    assert outs[0][1] == outs[1][1] == outs[0][2]
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+
+
+def test_max_iterations_semantics():
+    """max_iterations reached: iterations == max, not converged, final mismatch from the last
+    evaluation (cpu_newton_raphson.cpp:100-174)."""
+    from gap_b200 import synth
+    from gap_b200.api import NewtonRaphson, PowerFlowConfig
+
+    net = synth.feeder_grid(0)
+    r = NewtonRaphson().solve_power_flow(net, None, PowerFlowConfig(tolerance=1e-8,
+                                                                    max_iterations=3,
+                                                                    base_power=1e6))
+    o = restate.nr_solve(net, tol=1e-8, max_iter=3, base_power=1e6)
+    assert not r.converged and r.iterations == 3 and not o["converged"]
+    assert r.final_mismatch == pytest.approx(o["final_mismatch"], rel=1e-9)
+    np.testing.assert_allclose(r.bus_voltages, o["v"], atol=1e-12)

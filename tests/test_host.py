@@ -1,0 +1,142 @@
+"""Host-side logic of libgapk.so, no GPU needed: the C ABI exports, the Y-bus pattern, and the
+symbolic block-LU schedule (executed on the CPU exactly as the kernels walk it)."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+import schedule_emu as E
+from helpers import network_of, parity_fixtures
+from oracle import restate
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared(header):
+    txt = open(os.path.join(ROOT, "include", header)).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(gapk_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    from gap_b200 import _native as N
+
+    L = N.lib()
+    names = declared("gapk.h")
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert L.gapk_version() >= 100
+
+
+@pytest.mark.parametrize("name", [n for n in parity_fixtures() if n != "kat_update"])
+def test_ybus_pattern_bit_exact(name):
+    from gap_b200.engine import YbusPlan
+
+    net, d = network_of(name)
+    p = YbusPlan.from_network(net)
+    assert np.array_equal(p.row_ptr, d["y_row_ptr"])
+    assert np.array_equal(p.col_idx, d["y_col_idx"])
+
+
+def _nets():
+    from gap_b200 import synth
+
+    out = [("c0", synth.feeder_grid(0), 1e6), ("tr300", synth.transmission_grid(3, n=300), 1e8)]
+    for n in ("kat_three_bus_pv", "kat_parallel_branches", "kat_appliances"):
+        net, d = network_of(n)
+        out.append((n, net, 1e6))
+    return out
+
+
+@pytest.mark.parametrize("case", _nets(), ids=lambda c: c[0])
+@pytest.mark.parametrize("jac", ["reference", "exact"])
+@pytest.mark.parametrize("ordering", ["mindeg", "natural"])
+def test_block_lu_schedule_solves_jacobian(case, jac, ordering):
+    from gap_b200.engine import NRPlan
+
+    name, net, base = case
+    rp, ci, vals = restate.ybus_pi(net)
+    ypu = vals * (net.u_rated[0] ** 2 / base)
+    plan = NRPlan(rp, ci, net.bus_type, jacobian=jac, ordering=ordering)
+    info = plan.info
+    assert info["n_vars"] == (net.n_bus - np.sum(net.bus_type == 2)) + np.sum(net.bus_type == 0)
+    rng = np.random.default_rng(0)
+    v = restate.flat_start(net) * np.exp(1j * rng.normal(0, 0.05, net.n_bus))
+    J, F, var, eq = E.jacobian_blocks(plan, rp, ci, ypu, v, net.bus_type, jac)
+    Ff = E.factor(plan, F)
+    b = rng.normal(size=J.shape[0])
+    nb = info["n_block"]
+    rhs = np.zeros((nb, 2))
+    for k in range(nb):
+        for c in range(2):
+            if eq[k, c] >= 0:
+                rhs[k, c] = b[eq[k, c]]
+    X = E.solve(plan, Ff, rhs)
+    x = np.zeros(J.shape[0])
+    for k in range(nb):
+        for c in range(2):
+            if var[k, c] >= 0:
+                x[var[k, c]] = X[k, c]
+    xr = np.linalg.solve(J, b)
+    assert np.max(np.abs(x - xr)) <= 1e-9 * np.max(np.abs(xr))
+
+
+def test_schedule_levels_respect_dependencies():
+    """Every factor pair reads slots owned by strictly lower elimination-tree levels."""
+    from gap_b200 import synth
+    from gap_b200.engine import NRPlan
+
+    net = synth.transmission_grid(5, n=800)
+    rp, ci, _ = restate.ybus_reference(net)
+    plan = NRPlan(rp, ci, net.bus_type)
+    nb = plan.info["n_block"]
+    nnzl = plan.info["nnz_l_blocks"]
+    lptr = plan.export("lptr")
+    lidx = plan.export("lidx")
+    lp = plan.export("level_ptr")
+    ln = plan.export("level_nodes")
+    level = np.zeros(nb, int)
+    for h in range(len(lp) - 1):
+        level[ln[lp[h]:lp[h + 1]]] = h
+    col_of = np.repeat(np.arange(nb), np.diff(lptr))
+    owner = np.concatenate([np.arange(nb), col_of, col_of])  # slot -> node whose level owns it
+    fa = plan.export("fa_ptr")
+    tg = plan.export("targets").reshape(-1, 4)
+    pr = plan.export("pairs").reshape(-1, 2)
+    for h in range(len(fa) - 1):
+        for t in range(fa[h], fa[h + 1]):
+            assert level[owner[tg[t, 0]]] == h
+            for p in range(tg[t, 1], tg[t, 2]):
+                assert level[owner[pr[p, 0]]] < h and level[owner[pr[p, 1]]] < h
+    # parents are above children
+    for k in range(nb):
+        if lptr[k + 1] > lptr[k]:
+            assert level[lidx[lptr[k]]] > level[k]
+
+
+def test_plan_rejects_bad_input():
+    from gap_b200 import _native as N
+    from gap_b200.engine import NRPlan
+
+    with pytest.raises(N.GapkError):
+        NRPlan(np.array([0, 1, 3]), np.array([0, 5, 1]), np.array([2, 0]))
+    with pytest.raises(N.GapkError):
+        NRPlan(np.array([0, 1, 2]), np.array([0, 1]), np.array([2, 7]))
+
+
+def test_synth_generators_deterministic():
+    from gap_b200 import synth
+
+    a = synth.transmission_grid(11, n=400)
+    b = synth.transmission_grid(11, n=400)
+    for f in ("from_id", "to_id", "r1", "x1", "b1", "k", "theta", "p", "q", "bus_type", "u_pu"):
+        assert np.array_equal(getattr(a, f), getattr(b, f))
+    assert abs(a.n_branch - 1.4 * 400) <= 2
+    assert np.sum(a.bus_type == 1) == 80 and np.sum(a.bus_type == 2) == 1
+    f, t, valid = a.branch_index()
+    br = synth.bridges(a.n_bus, f, t)
+    out = synth.n_minus_1(a, 20)
+    assert len(out) == 20 and not br[out].any()

@@ -1,0 +1,88 @@
+"""The oracle (CPU restatement) pinned against the reference's own outputs: golden vectors
+generated by tests/golden/make_golden.py from the reference CPU path and from the
+power-grid-model outputs shipped with the reference's tests."""
+
+import numpy as np
+import pytest
+
+from helpers import fixture_names, load, network_of, net_from, parity_fixtures
+from oracle import restate
+
+FIX = [n for n in parity_fixtures() if n != "kat_update"]
+
+
+@pytest.mark.parametrize("name", FIX)
+def test_ybus_restatement_bit_exact(name):
+    net, d = network_of(name)
+    rp, ci, va = restate.ybus_reference(net)
+    assert np.array_equal(rp, d["y_row_ptr"])
+    assert np.array_equal(ci, d["y_col_idx"])
+    assert np.array_equal(va.view(np.float64), d["y_values"].view(np.float64))
+
+
+@pytest.mark.parametrize("name", FIX)
+def test_nr_restatement_matches_reference(name):
+    net, d = network_of(name)
+    base = float(d["base_power"])
+    r = restate.nr_solve(net, tol=1e-8, max_iter=20, base_power=base)
+    assert r["converged"] == bool(d["ref_converged"])
+    assert abs(r["iterations"] - int(d["ref_iterations"])) <= 1
+    if r["converged"]:
+        assert np.max(np.abs(np.abs(r["v"]) - np.abs(d["ref_v"]))) < 1e-10
+        assert np.max(np.abs(np.angle(r["v"]) - np.angle(d["ref_v"]))) < 1e-10
+
+
+@pytest.mark.parametrize("name", fixture_names("pgm_"))
+def test_reference_and_restatement_vs_power_grid_model(name):
+    """The reference's own acceptance criterion (tests/pgm_validation/test_pgm_validation.py:38-43):
+    |V| within 5e-6 pu of the power-grid-model solution."""
+    net, d = network_of(name)
+    assert np.max(np.abs(np.abs(d["ref_v"]) - d["pgm_u_pu"])) < 5e-6
+    r = restate.nr_solve(net, tol=1e-8, max_iter=20, base_power=float(d["base_power"]))
+    assert np.max(np.abs(np.abs(r["v"]) - d["pgm_u_pu"])) < 5e-6
+
+
+@pytest.mark.parametrize("name", fixture_names("kat_"))
+def test_mismatch_restatement(name):
+    if name == "kat_update":
+        pytest.skip("no mismatch vectors")
+    net, d = network_of(name)
+    Y = restate.ybus_reference(net)
+    s_spec = net.specified_power(100e6)
+    for k in ("0", "1"):
+        v = d["mm_v" + k]
+        f = restate.mismatch(net.bus_type, restate.power_injections(*Y, v), s_spec) * 100e6
+        np.testing.assert_allclose(f, d["mm_f" + k], rtol=1e-12, atol=1e-9)
+
+
+def test_ybus_update_restatement():
+    d = load("kat_update")
+    net = net_from(d)
+    ch = net_from(d, "ch_")
+    Y = restate.ybus_reference(net)
+    rp, ci, va = restate.ybus_update_reference(Y, ch)
+    assert np.array_equal(rp, d["y_row_ptr"]) and np.array_equal(ci, d["y_col_idx"])
+    np.testing.assert_allclose(va, d["y_values"], rtol=1e-14, atol=1e-14)
+
+
+@pytest.mark.parametrize("name", fixture_names("lu_"))
+def test_lu_reference_solutions(name):
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    d = load(name)
+    n = len(d["row_ptr"]) - 1
+    A = sp.csr_matrix((d["values"], d["col_idx"], d["row_ptr"]), shape=(n, n))
+    x = spla.spsolve(A.tocsc(), d["rhs"])
+    assert int(d["ref_status"]) == 0
+    np.testing.assert_allclose(x, d["ref_x"], rtol=1e-10, atol=1e-12)
+
+
+def test_c0_generator_matches_fixture():
+    from gap_b200 import synth
+
+    for seed in range(5):
+        d = load(f"c0_seed{seed}")
+        net = synth.feeder_grid(seed)
+        for f in ("from_id", "to_id", "r1", "x1", "p", "q", "bus_type"):
+            assert np.array_equal(getattr(net, f), d["net_" + f]), f
