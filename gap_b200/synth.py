@@ -61,12 +61,16 @@ def feeder_grid(seed: int = 0, n: int = 200, tie_frac: float = 0.10) -> Network:
 
 TRANSMISSION_KV = 138.0
 BASE_MVA = 100.0
+# Per-bus loads are p ~ U[0,1] * LOAD_SCALE pu.  With LOAD_SCALE = 1 (0-100 MW at every bus of
+# a 100 MVA-base grid with x ~ U[0.01,0.2]) no power-flow solution exists at 10k buses: the
+# FP64 oracle's Newton iteration collapses the voltages; see the generator's notes.
+LOAD_SCALE = 0.1
 
 
 def transmission_grid(seed: int = 0, n: int = 10_000, mean_degree: float = 2.8,
                       trafo_frac: float = 0.10, pv_frac: float = 0.20,
-                      shunt_frac: float = 0.02, load_scale: float = 1.0,
-                      pv_gen_frac: float = 1.0) -> Network:
+                      shunt_frac: float = 0.02, load_scale: float = LOAD_SCALE,
+                      cover_hops: int = 2) -> Network:
     """Transmission-like grid, per-unit data on a 100 MVA base converted to Ohm / S at
     138 kV so that the reference's single-voltage-base per-unit step recovers them.
 
@@ -74,12 +78,15 @@ def transmission_grid(seed: int = 0, n: int = 10_000, mean_degree: float = 2.8,
     joins the nearest of the buses 0..i-1 among its k-nearest candidates, else a random
     earlier bus); extra ties (random bus, random one of its 6 nearest neighbours, until
     m = round(mean_degree*n/2)); per branch x ~ U[0.01,0.2], r = x / U[5,15], b ~ U[0,0.05];
-    transformer flags (trafo_frac of branches), tap ~ U[0.95,1.05], shift ~ U[0,10] deg (tap
-    branches carry b = 0); PV set (pv_frac of non-slack buses) and |V| setpoints
-    ~ U[0.98,1.05]; shunt set (shunt_frac of buses) with b ~ U[-0.05,0.05] pu; loads
-    p ~ U[0,1] pu * load_scale, q = U[0.1,0.4] p.  PV generation: pv_gen_frac of the total
-    load, split over PV buses in proportion to U[0.5,1.5] weights.  The slack is the bus
-    closest to the centre of the square, at 1.0 pu."""
+    transformer set (round(trafo_frac*m) branches drawn from the bridges first, then from the
+    other branches), tap ~ U[0.95,1.05], shift ~ U[0,10] deg (transformers carry b = 0); PV placement (random order, a bus becomes PV while it is more than
+    cover_hops hops from every voltage-controlled bus, then random top-up to pv_frac of the
+    buses) and |V| setpoints ~ U[0.98,1.05]; shunt set (shunt_frac of buses) with
+    b ~ U[-0.05,0.05] pu; loads p ~ U[0,1] pu * load_scale, q = U[0.1,0.4] p.  PV generation
+    is local: each bus's load is assigned to its nearest voltage-controlled bus (multi-source
+    BFS in hops) and every PV bus generates its region's load; the slack supplies its own
+    region and the losses.  The slack is the bus closest to the centre of the square, at
+    1.0 pu."""
     from scipy.spatial import cKDTree
 
     rng = np.random.default_rng(seed)
@@ -119,20 +126,60 @@ def transmission_grid(seed: int = 0, n: int = 10_000, mean_degree: float = 2.8,
     x_pu = rng.uniform(0.01, 0.2, size=m)
     r_pu = x_pu / rng.uniform(5.0, 15.0, size=m)
     b_pu = rng.uniform(0.0, 0.05, size=m)
-    is_tr = rng.random(m) < trafo_frac
+    # transformers sit on radial connections: drawn from the bridge branches (a phase shift
+    # there rotates the angles behind it instead of driving loop flow), then from the rest
+    is_br = bridges(n, frm, to)
+    n_tr = int(round(trafo_frac * m))
+    cand = rng.permutation(np.nonzero(is_br)[0])
+    other = rng.permutation(np.nonzero(~is_br)[0])
+    pick = np.concatenate([cand, other])[:n_tr]
+    is_tr = np.zeros(m, bool)
+    is_tr[pick] = True
     tap = np.where(is_tr, rng.uniform(0.95, 1.05, size=m), 1.0)
     shift = np.where(is_tr, np.deg2rad(rng.uniform(0.0, 10.0, size=m)), 0.0)
     b_pu = np.where(is_tr, 0.0, b_pu)
     slack = int(np.argmin(np.sum((xy - 0.5) ** 2, axis=1)))
-    order = rng.permutation(n)
-    order = order[order != slack]
+    adj = [[] for _ in range(n)]
+    for a, b in zip(frm, to):
+        adj[a].append(b)
+        adj[b].append(a)
+    # PV placement: buses in random order become PV while they are more than `cover_hops`
+    # hops from every voltage-controlled bus (slack included), then the PV set is topped up
+    # to pv_frac of the buses at random.
     n_pv = int(round(pv_frac * n))
-    pv = order[:n_pv]
+    dist = np.full(n, np.iinfo(np.int64).max)
+    is_pv = np.zeros(n, bool)
+
+    def cover(src):
+        dist[src] = 0
+        frontier = [src]
+        for d in range(1, cover_hops + 1):
+            nxt = []
+            for u in frontier:
+                for w in adj[u]:
+                    if dist[w] > d:
+                        dist[w] = d
+                        nxt.append(w)
+            frontier = nxt
+
+    cover(slack)
+    order = rng.permutation(n)
+    placed = 0
+    for v in order:
+        if placed >= n_pv:
+            break
+        if v != slack and dist[v] > cover_hops:
+            is_pv[v] = True
+            placed += 1
+            cover(int(v))
+    rest = np.array([v for v in rng.permutation(n) if v != slack and not is_pv[v]], np.int64)
+    is_pv[rest[: max(0, n_pv - int(is_pv.sum()))]] = True
+    pv = np.nonzero(is_pv)[0]
     bt = np.full(n, PQ, np.int32)
     bt[pv] = PV
     bt[slack] = SLACK
     vset = np.ones(n)
-    vset[pv] = rng.uniform(0.98, 1.05, size=n_pv)
+    vset[pv] = rng.uniform(0.98, 1.05, size=len(pv))
     n_sh = int(round(shunt_frac * n))
     sh_bus = rng.permutation(n)[:n_sh]
     sh_b = rng.uniform(-0.05, 0.05, size=n_sh)
@@ -140,9 +187,27 @@ def transmission_grid(seed: int = 0, n: int = 10_000, mean_degree: float = 2.8,
     q_load = rng.uniform(0.1, 0.4, size=n) * p_load
     p_load[slack] = 0.0
     q_load[slack] = 0.0
-    w = rng.uniform(0.5, 1.5, size=n_pv)
+    # local dispatch: every bus's load is served by its nearest (in hops) voltage-controlled
+    # bus; each PV bus generates the load of its region, the slack covers its own region and
+    # the losses
+    owner = np.full(n, -1, np.int64)
+    src = [slack] + [int(v) for v in pv]
+    for s_ in src:
+        owner[s_] = s_
+    frontier = list(src)
+    while frontier:
+        nxt = []
+        for u in frontier:
+            for w in adj[u]:
+                if owner[w] < 0:
+                    owner[w] = owner[u]
+                    nxt.append(w)
+        frontier = nxt
+    owner[owner < 0] = slack
+    region = np.zeros(n)
+    np.add.at(region, owner, p_load)
     p_gen = np.zeros(n)
-    p_gen[pv] = pv_gen_frac * p_load.sum() * w / w.sum()
+    p_gen[pv] = region[pv]
     u = TRANSMISSION_KV * 1e3
     zb = u * u / (BASE_MVA * 1e6)
     sbase = BASE_MVA * 1e6
@@ -222,3 +287,33 @@ def n_minus_1(net: Network, count: int, seed: int = 2) -> np.ndarray:
 def grid_sizes(count: int, lo: int = 500, hi: int = 20_000, seed: int = 3) -> np.ndarray:
     rng = np.random.default_rng(seed)
     return np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), size=count))).astype(int)
+
+
+def dc_start(net: Network, base_power: float = BASE_MVA * 1e6, s_spec=None) -> np.ndarray:
+    """Initial voltages for the transmission workloads: angles from a DC power flow
+    (B' theta = P + phase-shift injections, x scaled by the tap ratio, slack angle 0),
+    magnitudes at the SLACK/PV setpoints and 1.0 for PQ buses.  Host-side input preparation
+    (scipy sparse solve); returns complex128 [n_bus]."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    f, t, valid = net.branch_index()
+    zb = float(net.u_rated[0]) ** 2 / base_power
+    ff, tt = f[valid], t[valid]
+    x = net.x1[valid] / zb * net.k[valid]
+    x = np.where(np.abs(x) > 1e-9, x, 1e-9)
+    b = 1.0 / x
+    sh = net.theta[valid]
+    n = net.n_bus
+    B = sp.coo_matrix((np.r_[b, b, -b, -b], (np.r_[ff, tt, ff, tt], np.r_[ff, tt, tt, ff])),
+                      shape=(n, n)).tocsr()
+    P = (net.specified_power(base_power) if s_spec is None else np.asarray(s_spec)).real
+    Ps = np.zeros(n)
+    np.add.at(Ps, ff, b * sh)
+    np.add.at(Ps, tt, -b * sh)
+    keep = net.bus_type != SLACK
+    ang = np.zeros(n)
+    if keep.any():
+        ang[keep] = spla.spsolve(B[keep][:, keep].tocsc(), (P + Ps)[keep])
+    vm = np.where(net.bus_type == PQ, 1.0, net.u_pu)
+    return vm * np.exp(1j * ang)

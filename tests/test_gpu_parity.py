@@ -174,8 +174,9 @@ def test_batched_scenarios_match_oracle(precision, refine):
                     torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
     plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
     b = NRBatch(plan, S, precision=precision, lanes=8)
+    v0 = np.repeat(synth.dc_start(net, base)[None], S, axis=0)
     r = b.solve(y, torch.as_tensor(s_spec, device="cuda"),
-                u_pu=torch.as_tensor(net.u_pu, device="cuda"), tol=1e-10, max_iter=30,
+                v_init=torch.as_tensor(v0, device="cuda"), tol=1e-10, max_iter=30,
                 policy="newton", refine=refine)
     torch.cuda.synchronize()
     st = r.status.cpu().numpy()
@@ -184,7 +185,7 @@ def test_batched_scenarios_match_oracle(precision, refine):
     Y = restate.ybus_pi(net)
     for s in (0, 7, 8, 18):
         o = restate.nr_solve(net, Y=Y, tol=1e-12, max_iter=30, base_power=base,
-                             policy="newton", jac="exact", s_spec=s_spec[s])
+                             policy="newton", jac="exact", s_spec=s_spec[s], v0=v0[s])
         assert o["converged"]
         assert np.max(np.abs(np.abs(V[s]) - np.abs(o["v"]))) < 1e-8
         assert np.max(np.abs(np.angle(V[s]) - np.angle(o["v"]))) < 1e-8
