@@ -37,7 +37,7 @@ EXPORTS = [
 
 
 class PlanOptions(C.Structure):
-    _fields_ = [("jacobian_mode", C.c_int), ("ordering", C.c_int)]
+    _fields_ = [("jacobian_mode", C.c_int), ("ordering", C.c_int), ("dense_min", C.c_int)]
 
 
 class PlanInfo(C.Structure):
@@ -45,7 +45,8 @@ class PlanInfo(C.Structure):
                 ("n_pv", C.c_int), ("n_slack", C.c_int), ("n_vars", C.c_int),
                 ("nnz_y", C.c_int), ("nnz_l_blocks", C.c_int), ("n_slots", C.c_int),
                 ("n_a_blocks", C.c_int), ("n_levels", C.c_int), ("n_pairs", C.c_int64),
-                ("n_rows_pairs", C.c_int64), ("max_level_width", C.c_int)]
+                ("n_rows_pairs", C.c_int64), ("max_level_width", C.c_int),
+                ("n_tail", C.c_int), ("n_schur_pairs", C.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -55,7 +55,11 @@ struct NRPlanHost {
     std::vector<int> fa_ptr, targets, fb_ptr, scale;
     std::vector<int> pairs;  // (left slot, right slot)
     int64_t n_pairs = 0;
-    // forward solve row lists: for node k, (L slot, node m) pairs over m with k in struct(m)
+    // dense tail: the last n_tail nodes (ns = nb - n_tail sparse nodes before them);
+    // schur[4*t..] = (slot, pair_begin, pair_end, block position r*n_tail + c)
+    int n_tail = 0, ns = 0;
+    std::vector<int> schur;
+    // forward solve row lists: for node k, (L slot, node m) pairs over sparse m, k in struct(m)
     std::vector<int> rptr, rlist;
     // reference variable order <-> node components: var_of[node*2+c] = reference index or -1
     std::vector<int> var_of_comp;
@@ -64,6 +68,6 @@ struct NRPlanHost {
 };
 
 bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx,
-                const int* bus_type, int jac_mode, int ordering, NRPlanHost& out);
+                const int* bus_type, int jac_mode, int ordering, int dense_min, NRPlanHost& out);
 
 }  // namespace gapk

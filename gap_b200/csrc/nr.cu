@@ -390,13 +390,15 @@ int gapk_nr_plan_create(int n_bus, int nnz_y, const int* h_y_row_ptr, const int*
     }
     int jac = opt ? opt->jacobian_mode : GAPK_JAC_REFERENCE;
     int ord = opt ? opt->ordering : GAPK_ORDER_MINDEG;
+    int dmin = opt ? opt->dense_min : 0;
+    if (dmin == 0) dmin = 16;
     if ((jac != 0 && jac != 1) || (ord != 0 && ord != 1)) {
         set_error("gapk_nr_plan_create: bad options");
         return GAPK_EINVAL;
     }
     auto p = std::make_unique<gapk_nr_plan_s>();
     try {
-        if (!analyze_nr(n_bus, nnz_y, h_y_row_ptr, h_y_col_idx, h_bus_type, jac, ord, p->h))
+        if (!analyze_nr(n_bus, nnz_y, h_y_row_ptr, h_y_col_idx, h_bus_type, jac, ord, dmin, p->h))
             return GAPK_EINVAL;
     } catch (std::bad_alloc const&) {
         set_error("gapk_nr_plan_create: host allocation failed");
@@ -433,6 +435,10 @@ int gapk_nr_plan_get_info(gapk_nr_plan p, gapk_nr_plan_info* info) {
     info->n_pairs = h.n_pairs;
     info->n_rows_pairs = h.nnz_l;
     info->max_level_width = h.max_level_width;
+    info->n_tail = h.n_tail;
+    int64_t sp = 0;
+    for (size_t t = 0; t + 3 < h.schur.size(); t += 4) sp += h.schur[t + 2] - h.schur[t + 1];
+    info->n_schur_pairs = sp;
     return GAPK_OK;
 }
 
@@ -470,6 +476,7 @@ int64_t gapk_nr_plan_export(gapk_nr_plan p, int what, int* h_buf) {
         case 18: v = &h.slot_a; break;
         case 19: v = &h.arow_ptr; break;
         case 20: v = &h.arow; break;
+        case 21: v = &h.schur; break;
         default:
             set_error("gapk_nr_plan_export: unknown selector");
             return GAPK_EINVAL;

@@ -127,7 +127,7 @@ inline int find_in(std::vector<int> const& lidx, int b, int e, int x) {
 }  // namespace
 
 bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx,
-                const int* bus_type, int jac_mode, int ordering, NRPlanHost& P) {
+                const int* bus_type, int jac_mode, int ordering, int dense_min, NRPlanHost& P) {
     P = NRPlanHost{};
     P.n_bus = n_bus;
     P.nnz_y = nnz_y;
@@ -217,27 +217,44 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
     P.n_slots = nb + 2 * nnzl;
     const int Lbase = nb, Ubase = nb + nnzl;
 
-    // elimination tree heights -> levels
-    std::vector<int> height(nb, 0);
-    for (int k = 0; k < nb; ++k) {
+    // ---- dense trailing block ----
+    // T = the longest run of trailing nodes whose columns are completely full
+    // (struct(k) = {k+1, ..., nb-1}).  When T >= dense_min those nodes are factorised as one
+    // dense 2T x 2T matrix per scenario; everything before them ("sparse part", ns nodes) is
+    // factorised block by block on the level schedule.
+    int T = 0;
+    for (int k = nb - 1; k >= 0; --k) {
+        if (P.lptr[k + 1] - P.lptr[k] == nb - 1 - k)
+            ++T;
+        else
+            break;
+    }
+    if (dense_min <= 0 || T < dense_min) T = 0;
+    const int ns = nb - T;
+    P.n_tail = T;
+    P.ns = ns;
+
+    // elimination-forest heights of the sparse nodes -> levels
+    std::vector<int> height(ns, 0);
+    for (int k = 0; k < ns; ++k) {
         if (P.lptr[k + 1] > P.lptr[k]) {
             int parent = P.lidx[P.lptr[k]];
-            height[parent] = std::max(height[parent], height[k] + 1);
+            if (parent < ns) height[parent] = std::max(height[parent], height[k] + 1);
         }
     }
-    int nlev = nb ? (*std::max_element(height.begin(), height.end()) + 1) : 0;
+    int nlev = ns ? (*std::max_element(height.begin(), height.end()) + 1) : 0;
     P.n_levels = nlev;
     P.node_level = height;
     P.level_ptr.assign(nlev + 1, 0);
-    for (int k = 0; k < nb; ++k) P.level_ptr[height[k] + 1]++;
+    for (int k = 0; k < ns; ++k) P.level_ptr[height[k] + 1]++;
     for (int h = 0; h < nlev; ++h) {
         P.max_level_width = std::max(P.max_level_width, P.level_ptr[h + 1]);
         P.level_ptr[h + 1] += P.level_ptr[h];
     }
-    P.level_nodes.resize(nb);
+    P.level_nodes.resize(ns);
     {
         std::vector<int> fp(P.level_ptr.begin(), P.level_ptr.end() - 1);
-        for (int k = 0; k < nb; ++k) P.level_nodes[fp[height[k]]++] = k;
+        for (int k = 0; k < ns; ++k) P.level_nodes[fp[height[k]]++] = k;
     }
 
     // Y sources per (row bus, col bus): rows of (col, index), sorted by col then index
@@ -303,7 +320,10 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
     P.scale.clear();
 
     // ---- numeric factorisation schedule (left-looking block Crout) ----
-    // Every node m contributes L(a,m) U(m,b) to target (a,b) for all a, b in struct(m).
+    // Every sparse node m contributes L(a,m) U(m,b) to target (a,b) for all a, b in struct(m).
+    // Targets owned by sparse nodes are computed on the level schedule; targets inside the
+    // dense tail receive their sparse contributions in one parallel Schur-complement pass
+    // (the tail's own contributions are the dense LU's business).
     std::vector<int64_t> cnt(P.n_slots + 1, 0);
     auto target_of = [&](int a, int b) -> int {
         if (a == b) return a;
@@ -314,7 +334,7 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
         int pos = find_in(P.lidx, P.lptr[b], P.lptr[b + 1], a);
         return pos < 0 ? -1 : Lbase + pos;
     };
-    for (int m = 0; m < nb; ++m) {
+    for (int m = 0; m < ns; ++m) {
         int b0 = P.lptr[m], e0 = P.lptr[m + 1];
         for (int ia = b0; ia < e0; ++ia)
             for (int ib = b0; ib < e0; ++ib) {
@@ -328,10 +348,14 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
     }
     for (int s = 0; s < P.n_slots; ++s) cnt[s + 1] += cnt[s];
     P.n_pairs = cnt[P.n_slots];
+    if (P.n_pairs > INT32_MAX / 2) {
+        set_error("factorisation schedule too large for 32-bit pair indices");
+        return false;
+    }
     std::vector<int> spairs(static_cast<size_t>(P.n_pairs) * 2);
     {
         std::vector<int64_t> fp(cnt.begin(), cnt.end() - 1);
-        for (int m = 0; m < nb; ++m) {
+        for (int m = 0; m < ns; ++m) {
             int b0 = P.lptr[m], e0 = P.lptr[m + 1];
             for (int ia = b0; ia < e0; ++ia)
                 for (int ib = b0; ib < e0; ++ib) {
@@ -342,8 +366,17 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
                 }
         }
     }
-    // group targets by owner level; phase A holds every slot (D, U row, L column) of the
-    // level's nodes, heaviest first; phase B scales the level's L columns by D^-1.
+    auto emit = [&](int s) {
+        int pb = static_cast<int>(P.pairs.size() / 2);
+        for (int64_t q = cnt[s]; q < cnt[s + 1]; ++q) {
+            P.pairs.push_back(spairs[2 * q]);
+            P.pairs.push_back(spairs[2 * q + 1]);
+        }
+        return std::pair<int, int>(pb, static_cast<int>(P.pairs.size() / 2));
+    };
+    // sparse part: group targets by owner level; phase A holds every slot (D, U row,
+    // L column) of the level's nodes, heaviest first; phase B scales the level's L columns
+    // by D^-1.
     P.fa_ptr.assign(nlev + 1, 0);
     P.fb_ptr.assign(nlev + 1, 0);
     P.targets.clear();
@@ -364,15 +397,10 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
             return (cnt[x + 1] - cnt[x]) > (cnt[y + 1] - cnt[y]);
         });
         for (int s : lvl_slots) {
-            int pb = static_cast<int>(P.pairs.size() / 2);
-            for (int64_t q = cnt[s]; q < cnt[s + 1]; ++q) {
-                P.pairs.push_back(spairs[2 * q]);
-                P.pairs.push_back(spairs[2 * q + 1]);
-            }
-            int pe = static_cast<int>(P.pairs.size() / 2);
+            auto pe = emit(s);
             P.targets.push_back(s);
-            P.targets.push_back(pb);
-            P.targets.push_back(pe);
+            P.targets.push_back(pe.first);
+            P.targets.push_back(pe.second);
             P.targets.push_back(s < nb ? 1 : 0);
         }
         P.fa_ptr[h + 1] = static_cast<int>(P.targets.size() / 4);
@@ -385,19 +413,30 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
         }
         P.fb_ptr[h + 1] = static_cast<int>(P.scale.size() / 2);
     }
-    if (P.n_pairs > INT32_MAX / 2) {
-        set_error("factorisation schedule too large for 32-bit pair indices");
-        return false;
+    // dense tail: (slot, pair_begin, pair_end, dense block position r*T + c)
+    P.schur.clear();
+    for (int k = ns; k < nb; ++k) {
+        auto pe = emit(k);
+        P.schur.insert(P.schur.end(), {k, pe.first, pe.second, (k - ns) * T + (k - ns)});
+        for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
+            int a = P.lidx[p];
+            pe = emit(Ubase + p);
+            P.schur.insert(P.schur.end(), {Ubase + p, pe.first, pe.second, (k - ns) * T + (a - ns)});
+            pe = emit(Lbase + p);
+            P.schur.insert(P.schur.end(), {Lbase + p, pe.first, pe.second, (a - ns) * T + (k - ns)});
+        }
     }
 
-    // ---- forward-solve row lists ----
+    // ---- forward-solve row lists (sparse columns only; the tail's own columns are in the
+    // dense factor) ----
     P.rptr.assign(nb + 1, 0);
-    for (int p = 0; p < nnzl; ++p) P.rptr[P.lidx[p] + 1]++;
+    for (int m = 0; m < ns; ++m)
+        for (int p = P.lptr[m]; p < P.lptr[m + 1]; ++p) P.rptr[P.lidx[p] + 1]++;
     for (int k = 0; k < nb; ++k) P.rptr[k + 1] += P.rptr[k];
-    P.rlist.assign(static_cast<size_t>(nnzl) * 2, 0);
+    P.rlist.assign(static_cast<size_t>(P.rptr[nb]) * 2, 0);
     {
         std::vector<int> fp(P.rptr.begin(), P.rptr.end() - 1);
-        for (int m = 0; m < nb; ++m)
+        for (int m = 0; m < ns; ++m)
             for (int p = P.lptr[m]; p < P.lptr[m + 1]; ++p) {
                 int k = P.lidx[p];
                 int q = fp[k]++;

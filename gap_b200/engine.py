@@ -123,20 +123,22 @@ def shunt_params(net: Network) -> np.ndarray:
 _EXPORT = dict(bus_of_node=0, node_pq=1, lptr=2, lidx=3, level_ptr=4, level_nodes=5,
                slot_info=6, slot_src_ptr=7, slot_src=8, fa_ptr=9, targets=10, pairs=11,
                fb_ptr=12, scale=13, rptr=14, rlist=15, var_of_comp=16, eq_of_comp=17,
-               slot_a=18, arow_ptr=19, arow=20)
+               slot_a=18, arow_ptr=19, arow=20, schur=21)
 
 
 class NRPlan:
     """Symbolic analysis of one (Y pattern, bus types) pair; shared by every batch and every
     scenario with that pattern.  Host-only until a batch uploads it."""
 
-    def __init__(self, row_ptr, col_idx, bus_type, jacobian="reference", ordering="mindeg"):
+    def __init__(self, row_ptr, col_idx, bus_type, jacobian="reference", ordering="mindeg",
+                 dense_min=0):
         L = N.lib()
         rp = N.i32(row_ptr)
         ci = N.i32(col_idx)
         bt = N.i32(bus_type)
         opt = N.PlanOptions(N.JAC_REFERENCE if jacobian == "reference" else N.JAC_EXACT,
-                            N.ORDER_MINDEG if ordering == "mindeg" else N.ORDER_NATURAL)
+                            N.ORDER_MINDEG if ordering == "mindeg" else N.ORDER_NATURAL,
+                            int(dense_min))
         h = C.c_void_p()
         N.check(L.gapk_nr_plan_create(C.c_int(len(rp) - 1), C.c_int(len(ci)), N.iptr(rp),
                                       N.iptr(ci), N.iptr(bt), C.byref(opt), C.byref(h)))

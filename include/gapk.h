@@ -113,6 +113,8 @@ typedef struct gapk_nr_batch_s* gapk_nr_batch;
 typedef struct {
     int jacobian_mode; /* GAPK_JAC_*                                                       */
     int ordering;      /* GAPK_ORDER_*                                                     */
+    int dense_min;     /* trailing fully-dense block of at least this many nodes is
+                          factorised densely (0 = default 16, < 0 = never)                 */
 } gapk_nr_plan_options;
 
 typedef struct {
@@ -127,6 +129,8 @@ typedef struct {
     int64_t n_pairs;      /* block multiply-adds of one numeric factorisation               */
     int64_t n_rows_pairs; /* block multiply-adds of one forward solve                       */
     int max_level_width;
+    int n_tail;           /* nodes in the dense trailing block (0 = none)                   */
+    int64_t n_schur_pairs; /* block multiply-adds of the sparse part into the dense block   */
 } gapk_nr_plan_info;
 
 int gapk_nr_plan_create(int n_bus, int nnz_y, const int* h_y_row_ptr, const int* h_y_col_idx,
@@ -140,7 +144,9 @@ int gapk_nr_plan_get_info(gapk_nr_plan p, gapk_nr_plan_info* info);
  *   4 level_ptr[n_levels+1]  5 level_nodes[n_block]  6 slot_info[n_slots*4]
  *   7 slot_src_ptr[n_slots+1] 8 slot_src[...]        9 fa_ptr[n_levels+1]
  *  10 targets[n_targets*4]  11 pairs[n_pairs*2]     12 fb_ptr[n_levels+1] 13 scale[n_b*2]
- *  14 rptr[n_block+1]       15 rlist[...*2]
+ *  14 rptr[n_block+1]       15 rlist[...*2]     16 var_of_comp[2*n_block]
+ *  17 eq_of_comp[2*n_block]  18 slot_a[n_slots]   19 arow_ptr[n_block+1] 20 arow[...*2]
+ *  21 schur[n_tail^2*4] (slot, pair_begin, pair_end, block position)
  * Returns the number of ints written (or needed when h_buf is NULL). */
 int64_t gapk_nr_plan_export(gapk_nr_plan p, int what, int* h_buf);
 

@@ -37,8 +37,11 @@ def jacobian_blocks(plan, row_ptr, col_idx, ypu, v, bus_type, mode):
 
 
 def factor(plan, F):
+    """Returns (F, D): factored slot storage of the sparse part and the dense tail's LU
+    (unit-lower L below the diagonal, U on and above it; None when there is no tail)."""
     F = F.copy()
-    L = plan.info["n_levels"]
+    info = plan.info
+    L = info["n_levels"]
     fa = plan.export("fa_ptr")
     tg = plan.export("targets").reshape(-1, 4)
     pr = plan.export("pairs").reshape(-1, 2)
@@ -55,13 +58,31 @@ def factor(plan, F):
             F[slot] = acc
         for t in range(fb[h], fb[h + 1]):
             F[sc[t, 0]] = F[sc[t, 0]] @ F[sc[t, 1]]
-    return F
+    T = info["n_tail"]
+    if T == 0:
+        return F, None
+    D = np.zeros((2 * T, 2 * T))
+    for slot, pb, pe, pos in plan.export("schur").reshape(-1, 4):
+        acc = F[slot].copy()
+        for p in range(pb, pe):
+            acc -= F[pr[p, 0]] @ F[pr[p, 1]]
+        r, c = divmod(pos, T)
+        D[2 * r:2 * r + 2, 2 * c:2 * c + 2] = acc
+    n = 2 * T
+    for j in range(n):
+        D[j + 1:, j] /= D[j, j]
+        D[j + 1:, j + 1:] -= np.outer(D[j + 1:, j], D[j, j + 1:])
+    return F, D
 
 
-def solve(plan, F, rhs_nodes):
-    nb = plan.info["n_block"]
-    nnzl = plan.info["nnz_l_blocks"]
-    L = plan.info["n_levels"]
+def solve(plan, FD, rhs_nodes):
+    F, D = FD
+    info = plan.info
+    nb = info["n_block"]
+    nnzl = info["nnz_l_blocks"]
+    T = info["n_tail"]
+    ns = nb - T
+    L = info["n_levels"]
     lp = plan.export("level_ptr")
     ln = plan.export("level_nodes")
     rptr = plan.export("rptr")
@@ -76,6 +97,19 @@ def solve(plan, F, rhs_nodes):
             for q in range(rptr[k], rptr[k + 1]):
                 acc -= F[rl[q, 0]] @ X[rl[q, 1]]
             X[k] = acc
+    if T:
+        for k in range(ns, nb):
+            acc = X[k].copy()
+            for q in range(rptr[k], rptr[k + 1]):
+                acc -= F[rl[q, 0]] @ X[rl[q, 1]]
+            X[k] = acc
+        y = X[ns:].reshape(-1).copy()
+        n = 2 * T
+        for i in range(n):
+            y[i] -= D[i, :i] @ y[:i]
+        for i in range(n - 1, -1, -1):
+            y[i] = (y[i] - D[i, i + 1:] @ y[i + 1:]) / D[i, i]
+        X[ns:] = y.reshape(T, 2)
     for h in range(L - 1, -1, -1):
         for t in range(lp[h], lp[h + 1]):
             k = ln[t]

@@ -54,13 +54,16 @@ def _nets():
 @pytest.mark.parametrize("case", _nets(), ids=lambda c: c[0])
 @pytest.mark.parametrize("jac", ["reference", "exact"])
 @pytest.mark.parametrize("ordering", ["mindeg", "natural"])
-def test_block_lu_schedule_solves_jacobian(case, jac, ordering):
+@pytest.mark.parametrize("dense_min", [0, 4, -1])
+def test_block_lu_schedule_solves_jacobian(case, jac, ordering, dense_min):
     from gap_b200.engine import NRPlan
 
     name, net, base = case
     rp, ci, vals = restate.ybus_pi(net)
     ypu = vals * (net.u_rated[0] ** 2 / base)
-    plan = NRPlan(rp, ci, net.bus_type, jacobian=jac, ordering=ordering)
+    plan = NRPlan(rp, ci, net.bus_type, jacobian=jac, ordering=ordering, dense_min=dense_min)
+    if dense_min == -1:
+        assert plan.info["n_tail"] == 0
     info = plan.info
     assert info["n_vars"] == (net.n_bus - np.sum(net.bus_type == 2)) + np.sum(net.bus_type == 0)
     rng = np.random.default_rng(0)
@@ -91,7 +94,7 @@ def test_schedule_levels_respect_dependencies():
 
     net = synth.transmission_grid(5, n=800)
     rp, ci, _ = restate.ybus_reference(net)
-    plan = NRPlan(rp, ci, net.bus_type)
+    plan = NRPlan(rp, ci, net.bus_type, dense_min=4)
     nb = plan.info["n_block"]
     nnzl = plan.info["nnz_l_blocks"]
     lptr = plan.export("lptr")
@@ -102,6 +105,8 @@ def test_schedule_levels_respect_dependencies():
     for h in range(len(lp) - 1):
         level[ln[lp[h]:lp[h + 1]]] = h
     col_of = np.repeat(np.arange(nb), np.diff(lptr))
+    ns = nb - plan.info["n_tail"]
+    level[ns:] = 10**6
     owner = np.concatenate([np.arange(nb), col_of, col_of])  # slot -> node whose level owns it
     fa = plan.export("fa_ptr")
     tg = plan.export("targets").reshape(-1, 4)
@@ -112,9 +117,17 @@ def test_schedule_levels_respect_dependencies():
             for p in range(tg[t, 1], tg[t, 2]):
                 assert level[owner[pr[p, 0]]] < h and level[owner[pr[p, 1]]] < h
     # parents are above children
-    for k in range(nb):
+    for k in range(ns):
         if lptr[k + 1] > lptr[k]:
             assert level[lidx[lptr[k]]] > level[k]
+    # Schur targets are tail slots and read only sparse-part slots
+    sch = plan.export("schur").reshape(-1, 4)
+    assert len(sch) == plan.info["n_tail"] ** 2
+    assert plan.info["n_tail"] > 0
+    for slot, pb, pe, pos in sch:
+        assert owner[slot] >= ns
+        for p in range(pb, pe):
+            assert owner[pr[p, 0]] < ns and owner[pr[p, 1]] < ns
 
 
 def test_plan_rejects_bad_input():
