@@ -71,7 +71,7 @@ struct gapk_nr_plan_s {
     bool uploaded = false;
     int device = -1;
     DevBuf d_yrp, d_ycol, d_bt, d_nob, d_si, d_ss, d_sa, d_lp, d_ln, d_fa, d_tg, d_pr, d_fb,
-        d_sc, d_lptr, d_lidx, d_rptr, d_rl, d_arp, d_ar, d_var, d_eq;
+        d_sc, d_lptr, d_lidx, d_rptr, d_rl, d_arp, d_ar, d_var, d_eq, d_schur;
     PlanDev dev{};
 
     int upload() {
@@ -102,6 +102,7 @@ struct gapk_nr_plan_s {
         up(d_ar, h.arow);
         up(d_var, h.var_of_comp);
         up(d_eq, h.eq_of_comp);
+        up(d_schur, h.schur);
         if (rc) return rc;
         cudaGetDevice(&device);
         dev.n_bus = h.n_bus;
@@ -112,6 +113,10 @@ struct gapk_nr_plan_s {
         dev.n_levels = h.n_levels;
         dev.n_a = h.n_a;
         dev.jac_mode = h.jac_mode;
+        dev.ns = h.ns;
+        dev.n_tail = h.n_tail;
+        dev.n_schur = static_cast<int>(h.schur.size() / 4);
+        dev.schur = d_schur.as<int4>();
         dev.y_row_ptr = d_yrp.as<int>();
         dev.y_col = d_ycol.as<int>();
         dev.bus_type = d_bt.as<int>();
@@ -140,8 +145,10 @@ struct gapk_nr_plan_s {
 struct gapk_nr_batch_s {
     gapk_nr_plan plan = nullptr;
     int n_scen = 0, sw = 8, G = 0, precision = 0, y_shared = 1, threads = 256, use_graph = 1;
-    DevBuf V, Sspec, Scalc, Y, F, A64, rhs, dx, res, X, mis, state, solving, singular, iters,
-        status, fmis, gsolve, giter, ctrl, tol;
+    DevBuf V, Sspec, Scalc, Y, F, A64, rhs, dx, res, X, Dt, mis, state, solving, singular,
+        iters, status, fmis, gsolve, giter, ctrl, tol;
+    int dense_w = 0;        // panel width of the dense-tail LU (0: no tail)
+    size_t dense_smem = 0;  // dynamic shared memory of k_dense_lu
     BatchDev dev{};
     // graph cache
     cudaGraph_t graph = nullptr;
@@ -161,6 +168,28 @@ inline unsigned blocks_for(long items, int threads) {
 }
 
 template <typename T, int SW>
+void launch_solve(gapk_nr_batch b, cudaStream_t st, const double2* rhs, double2* out, int acc) {
+    PlanDev const& P = b->plan->dev;
+    BatchDev const& B = b->dev;
+    k_solve_fwd<T, SW><<<b->G, b->threads, 0, st>>>(P, B, rhs);
+    if (P.n_tail > 0)
+        k_dense_solve<T, SW><<<b->G * SW, 256, 2 * P.n_tail * sizeof(T), st>>>(P, B, out, acc);
+    k_solve_bwd<T, SW><<<b->G, b->threads, 0, st>>>(P, B, out, acc);
+}
+
+template <typename T, int SW>
+void launch_factor(gapk_nr_batch b, cudaStream_t st) {
+    PlanDev const& P = b->plan->dev;
+    BatchDev const& B = b->dev;
+    k_factor<T, SW><<<b->G, b->threads, 0, st>>>(P, B);
+    if (P.n_tail > 0) {
+        dim3 gs(blocks_for((long)P.n_schur * SW, 256), b->G);
+        k_schur<T, SW><<<gs, 256, 0, st>>>(P, B);
+        k_dense_lu<T><<<b->G * SW, 256, b->dense_smem, st>>>(B, 2 * P.n_tail, b->dense_w);
+    }
+}
+
+template <typename T, int SW>
 void launch_body(gapk_nr_batch b, cudaStream_t st, int use_cond, cudaGraphConditionalHandle h) {
     PlanDev const& P = b->plan->dev;
     BatchDev const& B = b->dev;
@@ -170,12 +199,12 @@ void launch_body(gapk_nr_batch b, cudaStream_t st, int use_cond, cudaGraphCondit
     k_check<SW><<<1, 1024, 0, st>>>(B, use_cond, h);
     dim3 gj(blocks_for((long)P.n_slots * SW, 256), G);
     k_jfill<T, SW><<<gj, 256, 0, st>>>(P, B);
-    k_factor<T, SW><<<G, b->threads, 0, st>>>(P, B);
-    k_solve<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs, B.dx, 0);
+    launch_factor<T, SW>(b, st);
+    launch_solve<T, SW>(b, st, B.rhs, B.dx, 0);
     for (int r = 0; r < b->cur_refine; ++r) {
         dim3 gr(blocks_for((long)P.nb * SW, 256), G);
         k_residual<SW><<<gr, 256, 0, st>>>(P, B);
-        k_solve<T, SW><<<G, b->threads, 0, st>>>(P, B, B.res, B.dx, 1);
+        launch_solve<T, SW>(b, st, B.res, B.dx, 1);
     }
     dim3 gu(blocks_for((long)P.n_bus * SW, 256), G);
     k_update<SW><<<gu, 256, 0, st>>>(P, B);
@@ -258,14 +287,14 @@ struct StageOp {
                 break;
             }
             case 2:
-                k_factor<T, SW><<<G, b->threads, 0, st>>>(P, B);
+                launch_factor<T, SW>(b, st);
                 break;
             case 3:
-                k_solve<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs, B.dx, 0);
+                launch_solve<T, SW>(b, st, B.rhs, B.dx, 0);
                 for (int r = 0; r < b->cur_refine; ++r) {
                     dim3 gr(blocks_for((long)P.nb * SW, 256), G);
                     k_residual<SW><<<gr, 256, 0, st>>>(P, B);
-                    k_solve<T, SW><<<G, b->threads, 0, st>>>(P, B, B.res, B.dx, 1);
+                    launch_solve<T, SW>(b, st, B.res, B.dx, 1);
                 }
                 break;
             case 4: {
@@ -536,6 +565,36 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     A(b->dx, L * nb * 16);
     A(b->res, L * nb * 16);
     A(b->X, L * nb * 2 * esz);
+    if (h.n_tail > 0) {
+        const size_t N = 2 * (size_t)h.n_tail;
+        const size_t smem_max = 232448 - 1024;  // opt-in shared memory per block, less static
+        b->dense_w = 0;
+        for (int w : {32, 24, 16, 8}) {
+            size_t bytes = (N * w + (size_t)w * ((N + 3) & ~size_t(3))) * esz;
+            if (bytes <= smem_max) {
+                b->dense_w = w;
+                b->dense_smem = bytes;
+                break;
+            }
+        }
+        if (b->dense_w == 0) {
+            set_error("dense tail of " + std::to_string(h.n_tail) +
+                      " nodes exceeds the shared-memory panel limit");
+            return GAPK_ERANGE;
+        }
+        A(b->Dt, L * N * N * esz);
+        cudaError_t e = b->precision == GAPK_PREC_FP64
+                            ? cudaFuncSetAttribute(k_dense_lu<double>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)b->dense_smem)
+                            : cudaFuncSetAttribute(k_dense_lu<float>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)b->dense_smem);
+        if (e != cudaSuccess) {
+            set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+            return GAPK_ECUDA;
+        }
+    }
     A(b->mis, L * 8);
     A(b->state, L * 4);
     A(b->solving, L * 4);
@@ -563,6 +622,7 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     d.dx = b->dx.as<double2>();
     d.res = b->res.as<double2>();
     d.X = b->X.p;
+    d.Dt = b->Dt.p;
     d.mis_bits = b->mis.as<unsigned long long>();
     d.state = b->state.as<int>();
     d.solving = b->solving.as<int>();
@@ -587,7 +647,7 @@ int64_t gapk_nr_batch_device_bytes(gapk_nr_batch b) {
     if (!b) return 0;
     int64_t s = 0;
     for (DevBuf* d : {&b->V, &b->Sspec, &b->Scalc, &b->Y, &b->F, &b->A64, &b->rhs, &b->dx,
-                      &b->res, &b->X, &b->mis, &b->state, &b->solving, &b->singular, &b->iters,
+                      &b->res, &b->X, &b->Dt, &b->mis, &b->state, &b->solving, &b->singular, &b->iters,
                       &b->status, &b->fmis, &b->gsolve, &b->giter, &b->ctrl, &b->tol})
         s += static_cast<int64_t>(d->bytes);
     return s;

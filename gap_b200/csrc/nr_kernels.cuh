@@ -24,6 +24,8 @@ enum { SC_CONVERGED = 0, SC_MAXITER = 1, SC_SINGULAR = 2, SC_NONFINITE = 3 };
 struct PlanDev {
     int n_bus, nb, nnz_y, n_slots, nnz_l, n_levels, n_a;
     int jac_mode;  // 0: reference (last duplicate, |x| <= 1e-12 dropped), 1: exact
+    int ns, n_tail, n_schur;  // sparse nodes, dense-tail nodes, Schur targets (= n_tail^2)
+    const int4* schur;        // (slot, pair_begin, pair_end, block position r*n_tail + c)
     const int* y_row_ptr;
     const int* y_col;
     const int* bus_type;
@@ -59,6 +61,7 @@ struct BatchDev {
     double2* dx;      // Newton correction per node [G][nb][SW]
     double2* res;     // refinement residual [G][nb][SW]
     void* X;          // triangular-solve work vector [G][nb][SW] (T2)
+    void* Dt;         // dense tail per scenario [G*SW][2*n_tail][2*n_tail] (T), row-major
     unsigned long long* mis_bits;  // [G*SW] max |Delta| bits of the current iteration
     int* state;       // [G*SW] 0 iterating, 1 done
     int* solving;     // [G*SW] correction + update this iteration
@@ -374,21 +377,231 @@ __global__ void k_factor(PlanDev P, BatchDev B) {
 }
 
 // ---------------------------------------------------------------------------------------
-// triangular solves: L y = b (unit lower), U x = y; x written as FP64 (optionally added)
+// dense tail: Schur-complement gather from the sparse part, blocked dense LU, dense solves
 // ---------------------------------------------------------------------------------------
 template <typename T, int SW>
-__global__ void k_solve(PlanDev P, BatchDev B, const double2* __restrict__ rhs, double2* out,
-                        int accumulate) {
+__global__ void __launch_bounds__(256) k_schur(PlanDev P, BatchDev B) {
+    const int g = blockIdx.y;
+    if (!B.gsolve[g]) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = tid / SW, lane = tid % SW;
+    if (t >= P.n_schur) return;
+    const int q = g * SW + lane;
+    const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
+    const int4 tg = P.schur[t];
+    Blk<T> acc = ldb(F + (size_t)tg.x * SW + lane);
+    for (int p = tg.y; p < tg.z; ++p) {
+        const int2 pr = P.pairs[p];
+        msub(acc, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
+    }
+    const int N = 2 * P.n_tail;
+    const int r = 2 * (tg.w / P.n_tail), c = 2 * (tg.w % P.n_tail);
+    T* D = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * N;
+    D[(size_t)r * N + c] = acc.a;
+    D[(size_t)r * N + c + 1] = acc.b;
+    D[(size_t)(r + 1) * N + c] = acc.c;
+    D[(size_t)(r + 1) * N + c + 1] = acc.d;
+}
+
+// Right-looking blocked LU without pivoting of one scenario's N x N tail (row-major, in
+// place): a panel of width w <= W <= 32 is factored in shared memory, U12 comes from a
+// triangular solve per column, and the trailing update uses 4x4 register tiles fed from the
+// shared panels.  Shared memory: panel [N][W] + U12 [W][ldu], ldu = N rounded up to 4.
+// A pivot below 1e-14 in magnitude (the reference LU's tolerance) marks the scenario
+// singular.
+template <typename T>
+__global__ void __launch_bounds__(256) k_dense_lu(BatchDev B, int N, int W) {
+    const int q = blockIdx.x;
+    if (q >= B.n_scen || !B.solving[q]) return;
+    T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * N;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* Pn = reinterpret_cast<T*>(smraw);
+    T* U = Pn + (size_t)N * W;
+    __shared__ int bad;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    for (int k0 = 0; k0 < N; k0 += W) {
+        const int w = min(W, N - k0);
+        const int m = N - k0;
+        for (int e = tid; e < m * w; e += nt) {
+            const int r = e / w, c = e % w;
+            Pn[r * W + c] = A[(size_t)(k0 + r) * N + k0 + c];
+        }
+        __syncthreads();
+        for (int j = 0; j < w; ++j) {
+            const T piv = Pn[j * W + j];
+            if (tid == 0 && !(fabs(piv) >= T(1e-14))) bad = 1;
+            const T inv = T(1) / piv;
+            for (int r = j + 1 + tid; r < m; r += nt) Pn[r * W + j] *= inv;
+            __syncthreads();
+            const int cols = w - j - 1;
+            if (cols > 0) {
+                for (int e = tid; e < (m - j - 1) * cols; e += nt) {
+                    const int r = j + 1 + e / cols, c = j + 1 + e % cols;
+                    Pn[r * W + c] = fma(-Pn[r * W + j], Pn[j * W + c], Pn[r * W + c]);
+                }
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < m * w; e += nt) {
+            const int r = e / w, c = e % w;
+            A[(size_t)(k0 + r) * N + k0 + c] = Pn[r * W + c];
+        }
+        const int n2 = N - k0 - w;
+        if (n2 > 0) {
+            const int ldu = (n2 + 3) & ~3;
+            for (int c = tid; c < n2; c += nt) {
+                T x[32];
+#pragma unroll
+                for (int r = 0; r < 32; ++r) {
+                    if (r < w) {
+                        T v = A[(size_t)(k0 + r) * N + k0 + w + c];
+#pragma unroll
+                        for (int qq = 0; qq < 32; ++qq)
+                            if (qq < r) v = fma(-Pn[r * W + qq], x[qq], v);
+                        x[r] = v;
+                        U[r * ldu + c] = v;
+                        A[(size_t)(k0 + r) * N + k0 + w + c] = v;
+                    }
+                }
+            }
+            // zero the padding columns of U12 so the 4-wide tiles read defined values
+            for (int e = tid; e < w * (ldu - n2); e += nt) U[(e / (ldu - n2)) * ldu + n2 + e % (ldu - n2)] = T(0);
+            __syncthreads();
+            const int tr = (m - w + 3) / 4, tc = (n2 + 3) / 4;
+            for (int tix = tid; tix < tr * tc; tix += nt) {
+                const int i0 = w + (tix / tc) * 4, c0 = (tix % tc) * 4;
+                T acc[4][4];
+#pragma unroll
+                for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc)
+                        acc[ii][cc] = (i0 + ii < m && c0 + cc < n2)
+                                          ? A[(size_t)(k0 + i0 + ii) * N + k0 + w + c0 + cc]
+                                          : T(0);
+                for (int r = 0; r < w; ++r) {
+                    T l[4], u[4];
+#pragma unroll
+                    for (int ii = 0; ii < 4; ++ii) l[ii] = (i0 + ii < m) ? Pn[(i0 + ii) * W + r] : T(0);
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc) u[cc] = U[r * ldu + c0 + cc];
+#pragma unroll
+                    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc) acc[ii][cc] = fma(-l[ii], u[cc], acc[ii][cc]);
+                }
+#pragma unroll
+                for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc)
+                        if (i0 + ii < m && c0 + cc < n2)
+                            A[(size_t)(k0 + i0 + ii) * N + k0 + w + c0 + cc] = acc[ii][cc];
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && bad) B.singular[q] = 1;
+}
+
+// Forward (unit L) then backward (U) substitution on one scenario's tail vector, blocked by
+// 32 rows: all warps form the dot products with the already-solved part, warp 0 solves the
+// 32x32 triangle with shuffles.
+template <typename T, int SW>
+__global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, double2* out,
+                                                     int accumulate) {
+    const int q = blockIdx.x;
+    if (q >= B.n_scen || !B.solving[q]) return;
+    const int g = q / SW, lane = q % SW;
+    const int N = 2 * P.n_tail;
+    const T* A = reinterpret_cast<const T*>(B.Dt) + (size_t)q * N * N;
+    Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* y = reinterpret_cast<T*>(smraw);
+    const int tid = threadIdx.x, wid = tid >> 5, ln = tid & 31, nw = blockDim.x >> 5;
+    for (int i = tid; i < P.n_tail; i += blockDim.x) {
+        const Vec2<T> v = ldv(X + (size_t)(P.ns + i) * SW + lane);
+        y[2 * i] = v.x;
+        y[2 * i + 1] = v.y;
+    }
+    __syncthreads();
+    for (int r0 = 0; r0 < N; r0 += 32) {
+        for (int rr = wid; rr < 32; rr += nw) {
+            const int row = r0 + rr;
+            if (row >= N) continue;
+            T acc = T(0);
+            for (int c = ln; c < r0; c += 32) acc = fma(A[(size_t)row * N + c], y[c], acc);
+#pragma unroll
+            for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+            if (ln == 0) y[row] -= acc;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            const int row = r0 + ln;
+            T v = row < N ? y[row] : T(0);
+            for (int j = 0; j < 32; ++j) {
+                const T vj = __shfl_sync(0xffffffffu, v, j);
+                if (ln > j && row < N && r0 + j < N) v = fma(-A[(size_t)row * N + r0 + j], vj, v);
+            }
+            if (row < N) y[row] = v;
+        }
+        __syncthreads();
+    }
+    const int last = ((N - 1) / 32) * 32;
+    for (int r0 = last; r0 >= 0; r0 -= 32) {
+        const int r1 = min(r0 + 32, N);
+        for (int rr = wid; rr < 32; rr += nw) {
+            const int row = r0 + rr;
+            if (row >= N) continue;
+            T acc = T(0);
+            for (int c = r1 + ln; c < N; c += 32) acc = fma(A[(size_t)row * N + c], y[c], acc);
+#pragma unroll
+            for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+            if (ln == 0) y[row] -= acc;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            const int row = r0 + ln;
+            T v = row < N ? y[row] : T(0);
+            for (int j = 31; j >= 0; --j) {
+                if (r0 + j >= N) continue;
+                if (ln == j) v = v / A[(size_t)row * N + row];
+                const T vj = __shfl_sync(0xffffffffu, v, j);
+                if (ln < j && row < N) v = fma(-A[(size_t)row * N + r0 + j], vj, v);
+            }
+            if (row < N) y[row] = v;
+        }
+        __syncthreads();
+    }
+    double2* O = out + (size_t)g * P.nb * SW;
+    for (int i = tid; i < P.n_tail; i += blockDim.x) {
+        const int k = P.ns + i;
+        stv(X + (size_t)k * SW + lane, Vec2<T>{y[2 * i], y[2 * i + 1]});
+        double2* o = O + (size_t)k * SW + lane;
+        if (accumulate) {
+            const double2 old = *o;
+            *o = make_double2(old.x + (double)y[2 * i], old.y + (double)y[2 * i + 1]);
+        } else {
+            *o = make_double2((double)y[2 * i], (double)y[2 * i + 1]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// sparse triangular solves: L y = b (unit lower) over the sparse levels, then every tail
+// node gathers its sparse contributions; U x = y over the sparse levels (descending) once
+// the dense tail is solved.  x is written as FP64 (optionally added to `out`).
+// ---------------------------------------------------------------------------------------
+template <typename T, int SW>
+__global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ rhs) {
     const int g = blockIdx.x;
     if (!B.gsolve[g]) return;
     const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
     Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
     const double2* R = rhs + (size_t)g * P.nb * SW;
-    double2* O = out + (size_t)g * P.nb * SW;
     const int lane = threadIdx.x % SW;
     const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
-    const int L = P.n_levels;
-    for (int h = 0; h < L; ++h) {
+    for (int h = 0; h < P.n_levels; ++h) {
         for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
             const int k = P.level_nodes[t];
             const double2 b = R[(size_t)k * SW + lane];
@@ -401,8 +614,28 @@ __global__ void k_solve(PlanDev P, BatchDev B, const double2* __restrict__ rhs, 
         }
         __syncthreads();
     }
+    for (int k = P.ns + e0; k < P.nb; k += ne) {
+        const double2 b = R[(size_t)k * SW + lane];
+        Vec2<T> acc = {(T)b.x, (T)b.y};
+        for (int q = P.rptr[k]; q < P.rptr[k + 1]; ++q) {
+            const int2 r = P.rlist[q];
+            msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
+        }
+        stv(X + (size_t)k * SW + lane, acc);
+    }
+}
+
+template <typename T, int SW>
+__global__ void k_solve_bwd(PlanDev P, BatchDev B, double2* out, int accumulate) {
+    const int g = blockIdx.x;
+    if (!B.gsolve[g]) return;
+    const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
+    Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
+    double2* O = out + (size_t)g * P.nb * SW;
+    const int lane = threadIdx.x % SW;
+    const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
     const int Ub = P.nb + P.nnz_l;
-    for (int h = L - 1; h >= 0; --h) {
+    for (int h = P.n_levels - 1; h >= 0; --h) {
         for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
             const int k = P.level_nodes[t];
             Vec2<T> acc = ldv(X + (size_t)k * SW + lane);
@@ -456,8 +689,8 @@ __global__ void __launch_bounds__(256) k_update(PlanDev P, BatchDev B) {
     const int i = tid / SW, lane = tid % SW;
     if (i >= n) return;
     const int q = g * SW + lane;
-    const bool real = q < B.n_scen;
-    if (real) {
+    if (q >= B.n_scen) return;  // padding lanes are never updated
+    {
         if (B.singular[q]) {
             // the reference keeps V unchanged when factorize() fails and runs to max_iter
             if (i == 0 && B.solving[q]) {
