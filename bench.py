@@ -1,0 +1,466 @@
+"""Benchmark: power-flow solves/s on B200 -- batched mixed-precision Newton-Raphson.
+
+Workload (one "step"): 1024 load scenarios (per-bus lognormal sigma 0.1) of the seeded
+10k-bus transmission-like grid (mean degree 2.8, 10 % tap / phase-shift transformers, 20 % PV,
+2 % shunts), solved together to max |mismatch| < 1e-8 pu: FP32 Jacobian factor and triangular
+solves with one FP64 iterative-refinement step, FP64 mismatch / update / convergence, the
+whole Newton loop on the device (CUDA graph with a device-side while node).  Weak scaling:
+every rank solves its own 1024 scenarios of the same grid.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` times the solve with inputs resident in HBM; `e2e`
+times the same call with host (pinned) inputs and results copied inside the timed region.
+The plain FP64 single-scenario solve of the same grid is reported beside it.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Power-flow solves/s on 1 B200: batched mixed-precision vs plain FP64 at 1e-8 pu"
+N_BUS = 10_000
+GRID_SEED = 0
+N_SCEN = 1024
+SIGMA = 0.1
+TOL = 1e-8
+MAX_ITER = 20
+BASE = 1e8
+
+
+def workload(rank: int):
+    import numpy as np
+
+    from gap_b200 import synth
+
+    net = synth.transmission_grid(GRID_SEED, n=N_BUS)
+    s_spec = synth.load_scenarios(net, N_SCEN, sigma=SIGMA, seed=1 + rank, base_power=BASE)
+    v0 = synth.dc_start(net, BASE)
+    return net, s_spec, np.repeat(v0[None], N_SCEN, axis=0)
+
+
+def config(extra=None):
+    c = {"workload": f"{N_SCEN} load scenarios x {N_BUS}-bus transmission grid (seed {GRID_SEED})",
+         "n_bus": N_BUS, "scenarios_per_gpu": N_SCEN, "load_sigma": SIGMA, "tol_pu": TOL,
+         "max_iter": MAX_ITER, "precision": "fp32 factor+solve, fp64 mismatch/update, 1 refine",
+         "policy": "newton", "start": "dc angles", "l2": "inputs larger than L2 (state > 300 MB)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------------------------------------
+# CPU baseline: the oracle's FP64 restatement (sparse LU), one scenario per process
+# ------------------------------------------------------------------------------------------
+
+def _cpu_solve(idx):
+    import numpy as np
+
+    from oracle import restate
+
+    net, s_spec, v0 = _CPU_STATE
+    o = restate.nr_solve(net, Y=_CPU_Y, tol=TOL, max_iter=MAX_ITER, base_power=BASE,
+                         policy="newton", jac="exact", s_spec=s_spec[idx], v0=v0[idx])
+    return bool(o["converged"])
+
+
+def _cpu_init():
+    global _CPU_STATE, _CPU_Y
+    from oracle import restate
+
+    _CPU_STATE = workload(0)
+    _CPU_Y = restate.ybus_pi(_CPU_STATE[0])
+
+
+def _warm(i):
+    time.sleep(0.5)
+    return i
+
+
+def make_ready(pool, cores):
+    """Runs one sleeping task per worker so every worker has finished its initializer
+    (workload build) before anything is timed."""
+    pool.map(_warm, range(cores), chunksize=1)
+
+
+def cpu_run(pool, sample_idx):
+    t0 = time.perf_counter()
+    ok = sum(pool.map(_cpu_solve, sample_idx))
+    return ok, time.perf_counter() - t0
+
+
+def make_pool():
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    return ctx.Pool(cores, initializer=_cpu_init), cores
+
+
+# ------------------------------------------------------------------------------------------
+# clocks
+# ------------------------------------------------------------------------------------------
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        import statistics
+
+        self.f.flush()
+        rows = []
+        try:
+            with open(self.f.name) as fh:
+                for line in fh:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                        rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------
+# algorithmic bytes per kernel launch ("Roofline accounting")
+# ------------------------------------------------------------------------------------------
+
+def algorithmic_bytes(kernel, info, n_scen, esz):
+    n, nb, nnz = info["n_bus"], info["n_block"], info["nnz_y"]
+    ns_slots = info["n_slots"]
+    T = info["n_tail"]
+    N = 2 * T
+    nnzl = info["nnz_l_blocks"]
+    blk = 4 * esz
+    S = n_scen
+    if kernel == "mismatch":
+        return nnz * 20 + 4 * (n + 1) + S * (n * 16 * 3 + nb * 16)
+    if kernel == "jacobian":
+        return nnz * 16 + ns_slots * 16 + S * (n * 32 + ns_slots * blk + info["n_a_blocks"] * 32)
+    if kernel == "schur":
+        # read the tail slots and the sparse-part blocks that feed them once, write the dense tail
+        return S * (T * T * blk + nnzl * blk + N * N * esz)
+    if kernel == "dense_lu":
+        return S * 2 * N * N * esz
+    if kernel == "dense_solve":
+        return S * N * N * esz
+    if kernel == "factor_sparse":
+        return S * 2 * (ns_slots - T * T) * blk
+    if kernel in ("solve_fwd", "solve_bwd"):
+        return S * (nnzl * blk + nb * 16 * 2)
+    if kernel == "update":
+        return S * (n * 32 + nb * 16)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------
+
+def run_ours(args, rank, world, device):
+    import numpy as np
+    import torch
+
+    from gap_b200 import _native as N
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+
+    def barrier():
+        if dist:
+            tdist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.SUM)
+        return float(t.item())
+
+    pool = cores = None
+    if rank == 0 and world == 1:
+        pool, cores = make_pool()  # spawn context: safe beside the CUDA context
+        make_ready(pool, cores)
+
+    net, s_np, v_np = workload(rank)
+    zb = float(net.u_rated[0]) ** 2 / BASE
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=N.YBUS_TAPS,
+                    scale=zb)[0]
+    t0 = time.perf_counter()
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
+    plan_s = time.perf_counter() - t0
+    info = plan.info
+    batch = NRBatch(plan, N_SCEN, precision="fp32", lanes=8, threads=1024)
+    s_dev = torch.as_tensor(s_np, device="cuda")
+    v_dev = torch.as_tensor(v_np, device="cuda")
+
+    def step():
+        return batch.solve(y, s_dev, v_init=v_dev, tol=TOL, max_iter=MAX_ITER, policy="newton",
+                           refine=1)
+
+    for _ in range(args.warmup):
+        r = step()
+    torch.cuda.synchronize()
+    loops = batch.loop_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(device) as clk:
+        barrier()
+        e0.record()
+        for _ in range(args.steps):
+            r = step()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+    ms = allmax(e0.elapsed_time(e1))
+    status = r.status.cpu().numpy()
+    iters = r.iterations.cpu().numpy()
+    conv = int((status == 0).sum())
+    conv_all = allsum(conv)
+    value = conv_all * args.steps / (ms / 1e3)
+
+    # e2e: host (pinned) inputs -> device -> solve -> host results, every step
+    s_h = torch.as_tensor(s_np).pin_memory()
+    v_h = torch.as_tensor(v_np).pin_memory()
+    vo_h = torch.empty((N_SCEN, net.n_bus), dtype=torch.complex128).pin_memory()
+    st_h = torch.empty(N_SCEN, dtype=torch.int32).pin_memory()
+    it_h = torch.empty(N_SCEN, dtype=torch.int32).pin_memory()
+    fm_h = torch.empty(N_SCEN, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        sd = s_h.to("cuda", non_blocking=True)
+        vd = v_h.to("cuda", non_blocking=True)
+        rr = batch.solve(y, sd, v_init=vd, tol=TOL, max_iter=MAX_ITER, policy="newton", refine=1)
+        vo_h.copy_(rr.v, non_blocking=True)
+        st_h.copy_(rr.status, non_blocking=True)
+        it_h.copy_(rr.iterations, non_blocking=True)
+        fm_h.copy_(rr.final_mismatch, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = allmax(e0.elapsed_time(e1))
+    conv_e2e = allsum(int((st_h.numpy() == 0).sum()))
+    h2d = 2 * N_SCEN * net.n_bus * 16
+    d2h = N_SCEN * net.n_bus * 16 + N_SCEN * (4 + 4 + 8)
+
+    # per-kernel times (CUDA events on the launching stream), after a fresh Jacobian
+    batch.stage_load(y, s_dev, v_init=v_dev, refine=1)
+    batch.stage("mismatch")
+    kt = {}
+    for name in NRBatch.KERNELS:
+        ts = []
+        for _ in range(3):
+            batch.stage("jacobian")
+            if name in ("schur", "dense_lu"):
+                batch.kernel("factor_sparse")
+            if name == "dense_lu":
+                batch.kernel("schur")
+            if name in ("solve_fwd", "dense_solve", "solve_bwd"):
+                batch.stage("factor")
+            torch.cuda.synchronize()
+            e0.record()
+            batch.kernel(name)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        kt[name] = sorted(ts)[1]
+    per_iter = {"mismatch": 1, "jacobian": 1, "factor_sparse": 1, "schur": 1, "dense_lu": 1,
+                "solve_fwd": 2, "dense_solve": 2, "solve_bwd": 2, "update": 1}
+    if info["n_tail"] == 0:
+        for k in ("schur", "dense_lu", "dense_solve"):
+            per_iter[k] = 0
+    share = {k: kt[k] * per_iter[k] for k in kt}
+    dom = max(share, key=share.get)
+    esz = 4
+    alg = algorithmic_bytes(dom, info, N_SCEN, esz)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg / (kt[dom] / 1e3) / 1e9
+    launches_per_iter = 6 + 3 * 2 + 1 + 1 if info["n_tail"] else 4 + 2 * 2 + 1 + 1
+    gpu_launches = args.steps * (2 + loops * launches_per_iter)
+
+    # plain FP64 single-scenario path on the same grid
+    single = NRBatch(plan, 1, precision="fp64", lanes=1, threads=512)
+    s1 = s_dev[:1].contiguous()
+    v1 = v_dev[:1].contiguous()
+    for _ in range(args.warmup):
+        rs = single.solve(y, s1, v_init=v1, tol=TOL, max_iter=MAX_ITER, policy="newton")
+    torch.cuda.synchronize()
+    reps = max(args.steps, 5)
+    e0.record()
+    for _ in range(reps):
+        rs = single.solve(y, s1, v_init=v1, tol=TOL, max_iter=MAX_ITER, policy="newton")
+    e1.record()
+    torch.cuda.synchronize()
+    single_ms = e0.elapsed_time(e1) / reps
+    single_ok = int(rs.status[0].item()) == 0
+    plain = {"value": (1.0 if single_ok else 0.0) * 1e3 / single_ms, "unit": "solves/s",
+             "ms_per_solve": single_ms, "iterations": int(rs.iterations[0].item()),
+             "converged": single_ok}
+
+    cpu = None
+    if pool is not None:
+        sample = list(range(2 * cores)) if cores <= 8 else list(range(cores))
+        ok, wall = cpu_run(pool, sample)
+        cpu = {"value": ok / wall, "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": f"{len(sample)} scenarios of the same workload, FP64 restatement "
+                         f"(scipy sparse LU), one process per core, {wall:.1f} s wall"}
+        pool.close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
+            "data": "synthetic (seeded generator, no external dataset)",
+            "config": config({"parallelism": f"scenario shards x{world}",
+                              "converged_per_step": conv_all,
+                              "max_iterations_run": int(iters.max()), "plan_seconds": plan_s}),
+            "e2e": {"value": conv_e2e * args.steps / (e2e_ms / 1e3), "unit": "solves/s",
+                    "h2d_bytes_per_step": h2d * world, "d2h_bytes_per_step": d2h * world},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "algorithmic_bytes_per_launch": alg,
+                         "launch_ms": kt[dom], "peak_source": "measured" if peaks else "fallback"},
+            "kernel_ms": kt, "kernel_share_ms_per_iter": share,
+            "plain_fp64_single": plain,
+            "batched_over_plain_fp64": value / plain["value"] if plain["value"] else None,
+            "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": gpu_launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# reference arm: the reference path on host cores (CPU restatement; see module docstring)
+# ------------------------------------------------------------------------------------------
+
+REF_NOTE = ("the reference's own CPU backend (dense Jacobian, unordered LU, ~n^4) cannot finish "
+            "one 10k-bus solve in bounded time (1000 buses: 134 s per LU factorisation), so the "
+            "reference arm runs the FP64 CPU restatement of its algorithm with a sparse LU")
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    pool, cores = make_pool()
+    make_ready(pool, cores)
+    for w in range(args.warmup):
+        cpu_run(pool, [w])
+    tot_ok = 0
+    tot_t = 0.0
+    for s in range(args.steps):
+        idx = [(s * cores + i) % N_SCEN for i in range(cores)]
+        ok, t = cpu_run(pool, idx)
+        tot_ok += ok
+        tot_t += t
+    pool.close()
+    v = tot_ok / tot_t
+    line = {
+        "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tot_t / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, no external dataset)", "config": config(),
+        "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": f"{cores} scenarios per step, one process per core; {REF_NOTE}"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+
+            tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -306,6 +306,34 @@ struct StageOp {
     }
 };
 template <typename T, int SW>
+struct KernelOp {
+    static void run(gapk_nr_batch b, int which, cudaStream_t st) {
+        PlanDev const& P = b->plan->dev;
+        BatchDev const& B = b->dev;
+        const int G = b->G;
+        switch (which) {
+            case 0: k_mismatch<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B); break;
+            case 1: k_jfill<T, SW><<<dim3(blocks_for((long)P.n_slots * SW, 256), G), 256, 0, st>>>(P, B); break;
+            case 2: k_factor<T, SW><<<G, b->threads, 0, st>>>(P, B); break;
+            case 3:
+                if (P.n_tail > 0)
+                    k_schur<T, SW><<<dim3(blocks_for((long)P.n_schur * SW, 256), G), 256, 0, st>>>(P, B);
+                break;
+            case 4:
+                if (P.n_tail > 0)
+                    k_dense_lu<T><<<G * SW, 256, b->dense_smem, st>>>(B, 2 * P.n_tail, b->dense_w);
+                break;
+            case 5: k_solve_fwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs); break;
+            case 6:
+                if (P.n_tail > 0)
+                    k_dense_solve<T, SW><<<G * SW, 256, 2 * P.n_tail * sizeof(T), st>>>(P, B, B.dx, 0);
+                break;
+            case 7: k_solve_bwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.dx, 0); break;
+            case 8: k_update<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B); break;
+        }
+    }
+};
+template <typename T, int SW>
 struct ToRefOp {
     static void run(gapk_nr_batch b, const double2* src, const int* map, int n_out, double sign,
                     double* dst, cudaStream_t st) {
@@ -716,6 +744,15 @@ int gapk_nr_stage_mismatch(gapk_nr_batch b, void* s) { return stage(b, 0, s); }
 int gapk_nr_stage_jacobian(gapk_nr_batch b, void* s) { return stage(b, 1, s); }
 int gapk_nr_stage_factor(gapk_nr_batch b, void* s) { return stage(b, 2, s); }
 int gapk_nr_stage_solve(gapk_nr_batch b, void* s) { return stage(b, 3, s); }
+
+int gapk_nr_stage_kernel(gapk_nr_batch b, int kernel, void* stream) {
+    if (!b || kernel < 0 || kernel > 8) {
+        set_error("gapk_nr_stage_kernel: bad arguments");
+        return GAPK_EINVAL;
+    }
+    dispatch_tsw<KernelOp>(b->precision, b->sw, b, kernel, static_cast<cudaStream_t>(stream));
+    return check_launch();
+}
 
 int gapk_nr_stage_get_correction(gapk_nr_batch b, double* d_dx, void* stream) {
     if (!b || !d_dx) return GAPK_EINVAL;

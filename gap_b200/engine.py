@@ -235,6 +235,14 @@ class NRBatch:
               "factor": "gapk_nr_stage_factor", "solve": "gapk_nr_stage_solve"}[name]
         N.check(getattr(N.lib(), fn)(self._h, _stream_ptr(stream)))
 
+    KERNELS = ("mismatch", "jacobian", "factor_sparse", "schur", "dense_lu", "solve_fwd",
+               "dense_solve", "solve_bwd", "update")
+
+    def kernel(self, name, stream=None):
+        """Launch one kernel of the loop body (timing / profiling)."""
+        N.check(N.lib().gapk_nr_stage_kernel(self._h, self.KERNELS.index(name),
+                                             _stream_ptr(stream)))
+
     def correction(self, stream=None):
         torch = _torch()
         nv = self.plan.info["n_vars"]

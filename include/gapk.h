@@ -205,6 +205,11 @@ int gapk_nr_stage_mismatch(gapk_nr_batch b, void* stream);
 int gapk_nr_stage_jacobian(gapk_nr_batch b, void* stream);
 int gapk_nr_stage_factor(gapk_nr_batch b, void* stream);
 int gapk_nr_stage_solve(gapk_nr_batch b, void* stream);
+/* One kernel of the loop body, for per-kernel timing and profiling:
+ *   0 mismatch  1 jacobian fill  2 sparse factor  3 Schur gather  4 dense LU
+ *   5 sparse forward solve  6 dense solve  7 sparse backward solve  8 update
+ * Kernels 3, 4 and 6 do nothing when the plan has no dense tail. */
+int gapk_nr_stage_kernel(gapk_nr_batch b, int kernel, void* stream);
 /* Newton correction of the last stage_solve, [n_scen][n_vars] doubles in the reference's
  * variable order (theta of non-slack buses, then |V| of PQ buses). */
 int gapk_nr_stage_get_correction(gapk_nr_batch b, double* d_dx, void* stream);
