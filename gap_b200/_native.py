@@ -32,7 +32,7 @@ EXPORTS = [
     "gapk_nr_solve", "gapk_nr_last_loop_count",
     "gapk_nr_stage_load", "gapk_nr_stage_mismatch", "gapk_nr_stage_jacobian",
     "gapk_nr_stage_factor", "gapk_nr_stage_solve", "gapk_nr_stage_get_correction",
-    "gapk_nr_stage_get_mismatch", "gapk_nr_stage_kernel",
+    "gapk_nr_stage_get_mismatch", "gapk_nr_stage_kernel", "gapk_nr_solve_noalloc",
 ]
 
 

@@ -769,3 +769,224 @@ int gapk_nr_stage_get_mismatch(gapk_nr_batch b, double* d_f, void* stream) {
 }
 
 }  // extern "C"
+
+// ===========================================================================================
+// Allocation-free single-scenario solve.
+//
+// Some callers cannot call cudaMalloc at solve time: code that runs while another library
+// holds the device in stream capture, hosts that hand out device memory only from their own
+// pools, and real-time loops that must not touch the allocator.  gapk_nr_solve_noalloc serves
+// them: it solves one scenario in FP64 with the same kernels as gapk_nr_solve, but every
+// buffer it needs (a copy of the plan's index lists and the whole Newton state) is carved out
+// of one file-scope device array of fixed size.  The caller passes only inputs and outputs.
+// ===========================================================================================
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB, held by every device
+                                                             // that loads the library
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  In host code the array's name
+// is only a host-side stand-in, so the address must come from cudaGetSymbolAddress, once per
+// device, with that device current.
+int noalloc_scratch_ptr(void** out) {
+    int dev = 0;
+    GAPK_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("gapk_nr_solve_noalloc: device index out of range");
+        return GAPK_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        GAPK_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        GAPK_CUDA_TRY(cudaFuncSetAttribute(k_dense_lu<double>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           232448 - 1024));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return GAPK_OK;
+}
+
+struct Carver {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        size_t o = off;
+        off += (bytes + 255) & ~size_t(255);
+        return o;
+    }
+};
+
+}  // namespace
+
+extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
+                                     const gapk_nr_outputs* out, void* stream) {
+    if (!p || !in || !in->d_y || !in->d_s_spec) {
+        set_error("gapk_nr_solve_noalloc: plan, d_y and d_s_spec are required");
+        return GAPK_EINVAL;
+    }
+    if (in->max_iterations < 0 || in->refine != 0 ||
+        (in->policy != GAPK_POLICY_REFERENCE && in->policy != GAPK_POLICY_NEWTON)) {
+        set_error("gapk_nr_solve_noalloc: bad max_iterations / policy, or refine != 0 "
+                  "(this entry point solves in FP64 only)");
+        return GAPK_EINVAL;
+    }
+    auto const& h = p->h;
+    const size_t n = h.n_bus, nb = h.nb, nnz = h.nnz_y, N = 2 * (size_t)h.n_tail;
+    // plan index lists copied into the scratch, in this order
+    std::vector<int> const* lists[] = {&p->y_row_ptr, &p->y_col, &h.bus_type, &h.node_of_bus,
+                                       &h.slot_info, &h.slot_src, &h.slot_a, &h.level_ptr,
+                                       &h.level_nodes, &h.fa_ptr, &h.targets, &h.pairs,
+                                       &h.fb_ptr, &h.scale, &h.lptr, &h.lidx, &h.rptr,
+                                       &h.rlist, &h.arow_ptr, &h.arow, &h.schur};
+    constexpr int kLists = sizeof(lists) / sizeof(lists[0]);
+    Carver c;
+    size_t loff[kLists];
+    for (int i = 0; i < kLists; ++i) loff[i] = c.take(lists[i]->size() * sizeof(int));
+    const size_t oV = c.take(n * 16), oS = c.take(n * 16), oSc = c.take(n * 16),
+                 oY = c.take(nnz * 16), oF = c.take((size_t)h.n_slots * 32),
+                 oRhs = c.take(nb * 16), oDx = c.take(nb * 16), oRes = c.take(nb * 16),
+                 oX = c.take(nb * 16), oDt = c.take(N * N * 8), oMis = c.take(8),
+                 oState = c.take(4), oSolv = c.take(4), oSing = c.take(4), oIt = c.take(4),
+                 oSt = c.take(4), oFm = c.take(8), oGs = c.take(4), oGi = c.take(4),
+                 oCtrl = c.take(8 * 4), oTol = c.take(8);
+    if (c.off > kNoAllocScratchBytes) {
+        set_error("gapk_nr_solve_noalloc: this grid needs " + std::to_string(c.off) +
+                  " bytes of working memory; the static scratch holds " +
+                  std::to_string(kNoAllocScratchBytes) + " bytes (32 MiB)");
+        return GAPK_ERANGE;
+    }
+    size_t dense_smem = 0;
+    int dense_w = 0;
+    if (h.n_tail > 0) {
+        for (int w : {32, 24, 16, 8}) {
+            size_t bytes = (N * w + (size_t)w * ((N + 3) & ~size_t(3))) * 8;
+            if (bytes <= 232448 - 1024) {
+                dense_w = w;
+                dense_smem = bytes;
+                break;
+            }
+        }
+        if (!dense_w) {
+            set_error("gapk_nr_solve_noalloc: dense tail exceeds the shared-memory panel limit");
+            return GAPK_ERANGE;
+        }
+    }
+    void* base = nullptr;
+    int rc = noalloc_scratch_ptr(&base);
+    if (rc) return rc;
+    unsigned char* B0 = static_cast<unsigned char*>(base);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (int i = 0; i < kLists; ++i)
+        if (!lists[i]->empty())
+            GAPK_CUDA_TRY(cudaMemcpyAsync(B0 + loff[i], lists[i]->data(),
+                                          lists[i]->size() * sizeof(int),
+                                          cudaMemcpyHostToDevice, st));
+    auto L = [&](int i) { return reinterpret_cast<const int*>(B0 + loff[i]); };
+    PlanDev P{};
+    P.n_bus = h.n_bus;
+    P.nb = h.nb;
+    P.nnz_y = h.nnz_y;
+    P.n_slots = h.n_slots;
+    P.nnz_l = h.nnz_l;
+    P.n_levels = h.n_levels;
+    P.n_a = h.n_a;
+    P.jac_mode = h.jac_mode;
+    P.ns = h.ns;
+    P.n_tail = h.n_tail;
+    P.n_schur = static_cast<int>(h.schur.size() / 4);
+    P.y_row_ptr = L(0);
+    P.y_col = L(1);
+    P.bus_type = L(2);
+    P.node_of_bus = L(3);
+    P.slot_info = reinterpret_cast<const int4*>(L(4));
+    P.slot_src = L(5);
+    P.slot_a = L(6);
+    P.level_ptr = L(7);
+    P.level_nodes = L(8);
+    P.fa_ptr = L(9);
+    P.targets = reinterpret_cast<const int4*>(L(10));
+    P.pairs = reinterpret_cast<const int2*>(L(11));
+    P.fb_ptr = L(12);
+    P.scale = reinterpret_cast<const int2*>(L(13));
+    P.lptr = L(14);
+    P.lidx = L(15);
+    P.rptr = L(16);
+    P.rlist = reinterpret_cast<const int2*>(L(17));
+    P.arow_ptr = L(18);
+    P.arow = reinterpret_cast<const int2*>(L(19));
+    P.schur = reinterpret_cast<const int4*>(L(20));
+    BatchDev D{};
+    D.n_scen = 1;
+    D.n_groups = 1;
+    D.sw = 1;
+    D.y_shared = 1;
+    D.V = reinterpret_cast<double2*>(B0 + oV);
+    D.Sspec = reinterpret_cast<double2*>(B0 + oS);
+    D.Scalc = reinterpret_cast<double2*>(B0 + oSc);
+    D.Y = reinterpret_cast<double2*>(B0 + oY);
+    D.F = B0 + oF;
+    D.A64 = nullptr;
+    D.rhs = reinterpret_cast<double2*>(B0 + oRhs);
+    D.dx = reinterpret_cast<double2*>(B0 + oDx);
+    D.res = reinterpret_cast<double2*>(B0 + oRes);
+    D.X = B0 + oX;
+    D.Dt = B0 + oDt;
+    D.mis_bits = reinterpret_cast<unsigned long long*>(B0 + oMis);
+    D.state = reinterpret_cast<int*>(B0 + oState);
+    D.solving = reinterpret_cast<int*>(B0 + oSolv);
+    D.singular = reinterpret_cast<int*>(B0 + oSing);
+    D.iters = reinterpret_cast<int*>(B0 + oIt);
+    D.status = reinterpret_cast<int*>(B0 + oSt);
+    D.final_mis = reinterpret_cast<double*>(B0 + oFm);
+    D.gsolve = reinterpret_cast<int*>(B0 + oGs);
+    D.giter = reinterpret_cast<int*>(B0 + oGi);
+    D.ctrl = reinterpret_cast<int*>(B0 + oCtrl);
+    D.tol = reinterpret_cast<double*>(B0 + oTol);
+    // control words and state start fresh on every call (the scratch keeps the last call's)
+    int ctrl[8] = {0, in->max_iterations, 1, in->policy, 0, 0, 0, 0};
+    GAPK_CUDA_TRY(cudaMemcpyAsync(D.ctrl, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, st));
+    double tol = in->tolerance;
+    GAPK_CUDA_TRY(cudaMemcpyAsync(D.tol, &tol, sizeof(double), cudaMemcpyHostToDevice, st));
+    k_load<1><<<blocks_for((long)n, 256), 256, 0, st>>>(
+        P, D, reinterpret_cast<const double2*>(in->d_y),
+        reinterpret_cast<const double2*>(in->d_s_spec),
+        reinterpret_cast<const double2*>(in->d_v_init), in->d_u_pu);
+    rc = check_launch();
+    if (rc) return rc;
+    const int thr = 512;
+    for (int it = 0; it < in->max_iterations; ++it) {
+        k_mismatch<1><<<blocks_for((long)n, 256), 256, 0, st>>>(P, D);
+        k_check<1><<<1, 1024, 0, st>>>(D, 0, cudaGraphConditionalHandle{});
+        k_jfill<double, 1><<<blocks_for((long)h.n_slots, 256), 256, 0, st>>>(P, D);
+        k_factor<double, 1><<<1, thr, 0, st>>>(P, D);
+        if (h.n_tail > 0) {
+            k_schur<double, 1><<<blocks_for((long)P.n_schur, 256), 256, 0, st>>>(P, D);
+            k_dense_lu<double><<<1, 256, dense_smem, st>>>(D, (int)N, dense_w);
+        }
+        k_solve_fwd<double, 1><<<1, thr, 0, st>>>(P, D, D.rhs);
+        if (h.n_tail > 0)
+            k_dense_solve<double, 1><<<1, 256, N * sizeof(double), st>>>(P, D, D.dx, 0);
+        k_solve_bwd<double, 1><<<1, thr, 0, st>>>(P, D, D.dx, 0);
+        k_update<1><<<blocks_for((long)n, 256), 256, 0, st>>>(P, D);
+        rc = check_launch();
+        if (rc) return rc;
+        int any = 0;
+        GAPK_CUDA_TRY(cudaMemcpyAsync(&any, D.ctrl + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+        GAPK_CUDA_TRY(cudaStreamSynchronize(st));
+        if (!any) break;
+    }
+    if (out) {
+        k_store<1><<<blocks_for((long)n, 256), 256, 0, st>>>(
+            P, D, reinterpret_cast<double2*>(out->d_v), out->d_iterations, out->d_status,
+            out->d_final_mismatch);
+        rc = check_launch();
+        if (rc) return rc;
+    }
+    return GAPK_OK;
+}

@@ -194,6 +194,23 @@ typedef struct {
 int gapk_nr_solve(gapk_nr_batch b, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
                   void* stream);
 
+/* Allocation-free variant of gapk_nr_solve for ONE scenario in FP64 (no counterpart in the
+ * reference).  For callers that may not allocate device memory while they solve -- code
+ * running inside another library's stream capture, hosts that own all device memory through
+ * their own pools, real-time loops that must not touch the allocator.  It calls no cudaMalloc,
+ * cudaFree or allocating library routine: the plan's index lists are copied into, and the
+ * whole Newton state lives in, one static 32 MiB device array that every GPU loading the
+ * library holds until the process exits.  Grids whose plan and state need more than 32 MiB
+ * (roughly beyond 10k buses) are rejected with GAPK_ERANGE.  `in` as for gapk_nr_solve with
+ * refine = 0 (d_y shared, d_s_spec / d_v_init / outputs for one scenario); the loop is
+ * host-driven (one stream synchronisation per iteration).  The first call on a device looks
+ * up the array's device address and sets a kernel attribute; make that first call before
+ * any stream capture.  All calls share the one array, so calls that overlap on the GPU (from
+ * several host threads or streams) race and corrupt each other; the array keeps the last
+ * call's contents, and every call reinitialises what it reads. */
+int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
+                          void* stream);
+
 /* Device counters of the last solve, copied to the host (synchronises the stream):
  * h_counters[0] = Newton iterations run by the device loop (max over scenarios). */
 int gapk_nr_last_loop_count(gapk_nr_batch b, void* stream, int* h_loops);
