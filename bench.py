@@ -227,7 +227,7 @@ def run_ours(args, rank, world, device):
         return float(t.item())
 
     pool = cores = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         pool, cores = make_pool()  # spawn context: safe beside the CUDA context
         make_ready(pool, cores)
 
@@ -436,7 +436,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scenarios", type=int, default=N_SCEN,
+                    help="scenarios per GPU (profiling runs use fewer; the headline uses 1024)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling)")
     args = ap.parse_args()
+    global N_SCEN
+    N_SCEN = args.scenarios
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
