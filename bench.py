@@ -431,6 +431,7 @@ def run_reference(args, rank, world):
 
 
 def main():
+    global N_SCEN
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -440,7 +441,6 @@ def main():
                     help="scenarios per GPU (profiling runs use fewer; the headline uses 1024)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling)")
     args = ap.parse_args()
-    global N_SCEN
     N_SCEN = args.scenarios
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
