@@ -597,8 +597,8 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
         const size_t N = 2 * (size_t)h.n_tail;
         const size_t smem_max = 232448 - 1024;  // opt-in shared memory per block, less static
         b->dense_w = 0;
-        for (int w : {32, 24, 16, 8}) {
-            size_t bytes = (N * w + (size_t)w * ((N + 3) & ~size_t(3))) * esz;
+        for (int w : {16, 8}) {
+            size_t bytes = 2 * (size_t)w * dense_ld((int)N) * esz;
             if (bytes <= smem_max) {
                 b->dense_w = w;
                 b->dense_smem = bytes;
@@ -610,7 +610,7 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
                       " nodes exceeds the shared-memory panel limit");
             return GAPK_ERANGE;
         }
-        A(b->Dt, L * N * N * esz);
+        A(b->Dt, L * N * dense_ld((int)N) * esz);
         cudaError_t e = b->precision == GAPK_PREC_FP64
                             ? cudaFuncSetAttribute(k_dense_lu<double>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -851,7 +851,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
     const size_t oV = c.take(n * 16), oS = c.take(n * 16), oSc = c.take(n * 16),
                  oY = c.take(nnz * 16), oF = c.take((size_t)h.n_slots * 32),
                  oRhs = c.take(nb * 16), oDx = c.take(nb * 16), oRes = c.take(nb * 16),
-                 oX = c.take(nb * 16), oDt = c.take(N * N * 8), oMis = c.take(8),
+                 oX = c.take(nb * 16), oDt = c.take(N * dense_ld((int)N) * 8), oMis = c.take(8),
                  oState = c.take(4), oSolv = c.take(4), oSing = c.take(4), oIt = c.take(4),
                  oSt = c.take(4), oFm = c.take(8), oGs = c.take(4), oGi = c.take(4),
                  oCtrl = c.take(8 * 4), oTol = c.take(8);
@@ -864,8 +864,8 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
     size_t dense_smem = 0;
     int dense_w = 0;
     if (h.n_tail > 0) {
-        for (int w : {32, 24, 16, 8}) {
-            size_t bytes = (N * w + (size_t)w * ((N + 3) & ~size_t(3))) * 8;
+        for (int w : {16, 8}) {
+            size_t bytes = 2 * (size_t)w * dense_ld((int)N) * 8;
             if (bytes <= 232448 - 1024) {
                 dense_w = w;
                 dense_smem = bytes;

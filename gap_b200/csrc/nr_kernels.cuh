@@ -61,7 +61,7 @@ struct BatchDev {
     double2* dx;      // Newton correction per node [G][nb][SW]
     double2* res;     // refinement residual [G][nb][SW]
     void* X;          // triangular-solve work vector [G][nb][SW] (T2)
-    void* Dt;         // dense tail per scenario [G*SW][2*n_tail][2*n_tail] (T), row-major
+    void* Dt;         // dense tail per scenario [G*SW][2*n_tail][dense_ld] (T), row-major
     unsigned long long* mis_bits;  // [G*SW] max |Delta| bits of the current iteration
     int* state;       // [G*SW] 0 iterating, 1 done
     int* solving;     // [G*SW] correction + update this iteration
@@ -379,6 +379,31 @@ __global__ void k_factor(PlanDev P, BatchDev B) {
 // ---------------------------------------------------------------------------------------
 // dense tail: Schur-complement gather from the sparse part, blocked dense LU, dense solves
 // ---------------------------------------------------------------------------------------
+// Row stride of the dense tail: N rounded up to 8, so that every 8-column group that starts
+// on a multiple of 8 stays inside its (padded) row.
+__host__ __device__ __forceinline__ int dense_ld(int N) { return (N + 7) & ~7; }
+
+template <typename T>
+struct V4 {
+    T v[4];
+};
+__device__ __forceinline__ V4<float> ld4(const float* p) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    return {{a.x, a.y, a.z, a.w}};
+}
+__device__ __forceinline__ V4<double> ld4(const double* p) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0];
+    const double2 b = reinterpret_cast<const double2*>(p)[1];
+    return {{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ void st4(float* p, V4<float> const& a) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.v[0], a.v[1], a.v[2], a.v[3]);
+}
+__device__ __forceinline__ void st4(double* p, V4<double> const& a) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(a.v[0], a.v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(a.v[2], a.v[3]);
+}
+
 template <typename T, int SW>
 __global__ void __launch_bounds__(256) k_schur(PlanDev P, BatchDev B) {
     const int g = blockIdx.y;
@@ -394,29 +419,31 @@ __global__ void __launch_bounds__(256) k_schur(PlanDev P, BatchDev B) {
         const int2 pr = P.pairs[p];
         msub(acc, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
     }
-    const int N = 2 * P.n_tail;
+    const int N = 2 * P.n_tail, ld = dense_ld(N);
     const int r = 2 * (tg.w / P.n_tail), c = 2 * (tg.w % P.n_tail);
-    T* D = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * N;
-    D[(size_t)r * N + c] = acc.a;
-    D[(size_t)r * N + c + 1] = acc.b;
-    D[(size_t)(r + 1) * N + c] = acc.c;
-    D[(size_t)(r + 1) * N + c + 1] = acc.d;
+    T* D = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
+    D[(size_t)r * ld + c] = acc.a;
+    D[(size_t)r * ld + c + 1] = acc.b;
+    D[(size_t)(r + 1) * ld + c] = acc.c;
+    D[(size_t)(r + 1) * ld + c + 1] = acc.d;
 }
 
-// Right-looking blocked LU without pivoting of one scenario's N x N tail (row-major, in
-// place): a panel of width w <= W <= 32 is factored in shared memory, U12 comes from a
-// triangular solve per column, and the trailing update uses 4x4 register tiles fed from the
-// shared panels.  Shared memory: panel [N][W] + U12 [W][ldu], ldu = N rounded up to 4.
+// Right-looking blocked LU without pivoting of one scenario's N x N tail (row-major, row
+// stride dense_ld(N), in place).  Each panel of width w <= W (W = 8 or 16) is held TRANSPOSED
+// in shared memory, PT[c][r] = A[k0+r][k0+c], so a column of the panel is contiguous; U12 sits
+// row-major beside it.  The trailing update gives each thread 4x8 register tiles: per k it
+// reads 4 rows of L21 (one vector load) and 8 columns of U12 (two vector loads) for 32 FMAs.
 // A pivot below 1e-14 in magnitude (the reference LU's tolerance) marks the scenario
-// singular.
+// singular.  Shared memory: 2 * W * dense_ld(N) elements.
 template <typename T>
 __global__ void __launch_bounds__(256) k_dense_lu(BatchDev B, int N, int W) {
     const int q = blockIdx.x;
     if (q >= B.n_scen || !B.solving[q]) return;
-    T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * N;
+    const int ld = dense_ld(N);
+    T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* Pn = reinterpret_cast<T*>(smraw);
-    T* U = Pn + (size_t)N * W;
+    T* PT = reinterpret_cast<T*>(smraw);
+    T* U = PT + (size_t)W * ld;
     __shared__ int bad;
     const int tid = threadIdx.x, nt = blockDim.x;
     if (tid == 0) bad = 0;
@@ -426,77 +453,88 @@ __global__ void __launch_bounds__(256) k_dense_lu(BatchDev B, int N, int W) {
         const int m = N - k0;
         for (int e = tid; e < m * w; e += nt) {
             const int r = e / w, c = e % w;
-            Pn[r * W + c] = A[(size_t)(k0 + r) * N + k0 + c];
+            PT[c * ld + r] = A[(size_t)(k0 + r) * ld + k0 + c];
         }
         __syncthreads();
         for (int j = 0; j < w; ++j) {
-            const T piv = Pn[j * W + j];
+            const T piv = PT[j * ld + j];
             if (tid == 0 && !(fabs(piv) >= T(1e-14))) bad = 1;
             const T inv = T(1) / piv;
-            for (int r = j + 1 + tid; r < m; r += nt) Pn[r * W + j] *= inv;
+            for (int r = j + 1 + tid; r < m; r += nt) PT[j * ld + r] *= inv;
             __syncthreads();
-            const int cols = w - j - 1;
-            if (cols > 0) {
-                for (int e = tid; e < (m - j - 1) * cols; e += nt) {
-                    const int r = j + 1 + e / cols, c = j + 1 + e % cols;
-                    Pn[r * W + c] = fma(-Pn[r * W + j], Pn[j * W + c], Pn[r * W + c]);
-                }
+            const int cols = w - j - 1, rows = m - j - 1;
+            for (int e = tid; e < rows * cols; e += nt) {
+                const int c = j + 1 + e / rows, r = j + 1 + e % rows;
+                PT[c * ld + r] = fma(-PT[j * ld + r], PT[c * ld + j], PT[c * ld + r]);
             }
             __syncthreads();
         }
         for (int e = tid; e < m * w; e += nt) {
             const int r = e / w, c = e % w;
-            A[(size_t)(k0 + r) * N + k0 + c] = Pn[r * W + c];
+            A[(size_t)(k0 + r) * ld + k0 + c] = PT[c * ld + r];
         }
         const int n2 = N - k0 - w;
         if (n2 > 0) {
-            const int ldu = (n2 + 3) & ~3;
-            for (int c = tid; c < n2; c += nt) {
-                T x[32];
+            // U12 = L11^-1 A12, one column per thread; pad columns of U12 to a multiple of 8
+            const int n2p = (n2 + 7) & ~7;
+            for (int c = tid; c < n2p; c += nt) {
+                T x[16];
 #pragma unroll
-                for (int r = 0; r < 32; ++r) {
+                for (int r = 0; r < 16; ++r) {
                     if (r < w) {
-                        T v = A[(size_t)(k0 + r) * N + k0 + w + c];
+                        T v = T(0);
+                        if (c < n2) {
+                            v = A[(size_t)(k0 + r) * ld + k0 + w + c];
 #pragma unroll
-                        for (int qq = 0; qq < 32; ++qq)
-                            if (qq < r) v = fma(-Pn[r * W + qq], x[qq], v);
+                            for (int qq = 0; qq < 16; ++qq)
+                                if (qq < r) v = fma(-PT[qq * ld + r], x[qq], v);
+                            A[(size_t)(k0 + r) * ld + k0 + w + c] = v;
+                        }
                         x[r] = v;
-                        U[r * ldu + c] = v;
-                        A[(size_t)(k0 + r) * N + k0 + w + c] = v;
+                        U[r * ld + c] = v;
                     }
                 }
             }
-            // zero the padding columns of U12 so the 4-wide tiles read defined values
-            for (int e = tid; e < w * (ldu - n2); e += nt) U[(e / (ldu - n2)) * ldu + n2 + e % (ldu - n2)] = T(0);
             __syncthreads();
-            const int tr = (m - w + 3) / 4, tc = (n2 + 3) / 4;
-            for (int tix = tid; tix < tr * tc; tix += nt) {
-                const int i0 = w + (tix / tc) * 4, c0 = (tix % tc) * 4;
-                T acc[4][4];
+            // trailing update, rows [w, m), columns [0, n2) of the trailing block
+            const int tr = (m - w + 3) / 4, tcn = n2p / 8;
+            for (int tix = tid; tix < tr * tcn; tix += nt) {
+                const int i0 = w + (tix / tcn) * 4, c0 = (tix % tcn) * 8;
+                T acc[4][8];
 #pragma unroll
-                for (int ii = 0; ii < 4; ++ii)
+                for (int ii = 0; ii < 4; ++ii) {
+                    if (i0 + ii < m) {
+                        const T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + w + c0;
+                        const V4<T> a = ld4(row), b = ld4(row + 4);
 #pragma unroll
-                    for (int cc = 0; cc < 4; ++cc)
-                        acc[ii][cc] = (i0 + ii < m && c0 + cc < n2)
-                                          ? A[(size_t)(k0 + i0 + ii) * N + k0 + w + c0 + cc]
-                                          : T(0);
+                        for (int cc = 0; cc < 4; ++cc) {
+                            acc[ii][cc] = a.v[cc];
+                            acc[ii][cc + 4] = b.v[cc];
+                        }
+                    } else {
+#pragma unroll
+                        for (int cc = 0; cc < 8; ++cc) acc[ii][cc] = T(0);
+                    }
+                }
                 for (int r = 0; r < w; ++r) {
-                    T l[4], u[4];
-#pragma unroll
-                    for (int ii = 0; ii < 4; ++ii) l[ii] = (i0 + ii < m) ? Pn[(i0 + ii) * W + r] : T(0);
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) u[cc] = U[r * ldu + c0 + cc];
+                    const V4<T> l = ld4(PT + r * ld + i0);
+                    const V4<T> u0 = ld4(U + r * ld + c0), u1 = ld4(U + r * ld + c0 + 4);
 #pragma unroll
                     for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) acc[ii][cc] = fma(-l[ii], u[cc], acc[ii][cc]);
+                        for (int cc = 0; cc < 4; ++cc) {
+                            acc[ii][cc] = fma(-l.v[ii], u0.v[cc], acc[ii][cc]);
+                            acc[ii][cc + 4] = fma(-l.v[ii], u1.v[cc], acc[ii][cc + 4]);
+                        }
                 }
 #pragma unroll
-                for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc)
-                        if (i0 + ii < m && c0 + cc < n2)
-                            A[(size_t)(k0 + i0 + ii) * N + k0 + w + c0 + cc] = acc[ii][cc];
+                for (int ii = 0; ii < 4; ++ii) {
+                    if (i0 + ii < m) {
+                        T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + w + c0;
+                        st4(row, V4<T>{{acc[ii][0], acc[ii][1], acc[ii][2], acc[ii][3]}});
+                        st4(row + 4, V4<T>{{acc[ii][4], acc[ii][5], acc[ii][6], acc[ii][7]}});
+                    }
+                }
             }
         }
         __syncthreads();
@@ -513,8 +551,8 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
     const int q = blockIdx.x;
     if (q >= B.n_scen || !B.solving[q]) return;
     const int g = q / SW, lane = q % SW;
-    const int N = 2 * P.n_tail;
-    const T* A = reinterpret_cast<const T*>(B.Dt) + (size_t)q * N * N;
+    const int N = 2 * P.n_tail, ld = dense_ld(N);
+    const T* A = reinterpret_cast<const T*>(B.Dt) + (size_t)q * N * ld;
     Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* y = reinterpret_cast<T*>(smraw);
@@ -530,7 +568,7 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
             const int row = r0 + rr;
             if (row >= N) continue;
             T acc = T(0);
-            for (int c = ln; c < r0; c += 32) acc = fma(A[(size_t)row * N + c], y[c], acc);
+            for (int c = ln; c < r0; c += 32) acc = fma(A[(size_t)row * ld + c], y[c], acc);
 #pragma unroll
             for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
             if (ln == 0) y[row] -= acc;
@@ -541,7 +579,7 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
             T v = row < N ? y[row] : T(0);
             for (int j = 0; j < 32; ++j) {
                 const T vj = __shfl_sync(0xffffffffu, v, j);
-                if (ln > j && row < N && r0 + j < N) v = fma(-A[(size_t)row * N + r0 + j], vj, v);
+                if (ln > j && row < N && r0 + j < N) v = fma(-A[(size_t)row * ld + r0 + j], vj, v);
             }
             if (row < N) y[row] = v;
         }
@@ -554,7 +592,7 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
             const int row = r0 + rr;
             if (row >= N) continue;
             T acc = T(0);
-            for (int c = r1 + ln; c < N; c += 32) acc = fma(A[(size_t)row * N + c], y[c], acc);
+            for (int c = r1 + ln; c < N; c += 32) acc = fma(A[(size_t)row * ld + c], y[c], acc);
 #pragma unroll
             for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
             if (ln == 0) y[row] -= acc;
@@ -565,9 +603,9 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
             T v = row < N ? y[row] : T(0);
             for (int j = 31; j >= 0; --j) {
                 if (r0 + j >= N) continue;
-                if (ln == j) v = v / A[(size_t)row * N + row];
+                if (ln == j) v = v / A[(size_t)row * ld + row];
                 const T vj = __shfl_sync(0xffffffffu, v, j);
-                if (ln < j && row < N) v = fma(-A[(size_t)row * N + r0 + j], vj, v);
+                if (ln < j && row < N) v = fma(-A[(size_t)row * ld + r0 + j], vj, v);
             }
             if (row < N) y[row] = v;
         }

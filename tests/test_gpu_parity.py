@@ -227,3 +227,44 @@ def test_max_iterations_semantics():
     assert not r.converged and r.iterations == 3 and not o["converged"]
     assert r.final_mismatch == pytest.approx(o["final_mismatch"], rel=1e-9)
     np.testing.assert_allclose(r.bus_voltages, o["v"], atol=1e-12)
+
+
+@pytest.mark.parametrize("precision,lanes,dense_min", [("fp64", 1, 0), ("fp32", 8, 0),
+                                                       ("fp64", 2, -1)])
+def test_dense_tail_correction_matches_sparse_solve(precision, lanes, dense_min):
+    """A grid whose elimination order ends in a large dense block (dense tail on the device)
+    against scipy; dense_min=-1 runs the same grid fully on the sparse schedule."""
+    torch = _torch()
+    import scipy.sparse.linalg as spla
+
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.transmission_grid(9, n=4000)
+    base = 1e8
+    zb = net.u_rated[0] ** 2 / base
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact", dense_min=dense_min)
+    assert (plan.info["n_tail"] > 50) == (dense_min == 0)
+    S = 3
+    rng = np.random.default_rng(11)
+    v = np.stack([synth.dc_start(net, base) * np.exp(1j * rng.normal(0, 0.01, net.n_bus))
+                  for _ in range(S)])
+    s_spec = np.repeat(net.specified_power(base)[None], S, axis=0)
+    b = NRBatch(plan, S, precision=precision, lanes=lanes)
+    b.stage_load(y, torch.as_tensor(s_spec, device="cuda"),
+                 v_init=torch.as_tensor(v, device="cuda"), refine=1 if precision == "fp32" else 0)
+    for st in ("mismatch", "jacobian", "factor", "solve"):
+        b.stage(st)
+    dx = b.correction().cpu().numpy()
+    ypu = y.cpu().numpy()
+    for s in range(S):
+        sc = restate.power_injections(yp.row_ptr, yp.col_idx, ypu, v[s])
+        fr = restate.mismatch(net.bus_type, sc, s_spec[s])
+        J = restate.jacobian(yp.row_ptr, yp.col_idx, ypu, v[s], net.bus_type, mode="exact",
+                             drop=False)
+        xr = spla.spsolve(J.tocsc(), -fr)
+        tol = 1e-10 if precision == "fp64" else 1e-6
+        assert np.max(np.abs(dx[s] - xr)) <= tol * np.max(np.abs(xr))
