@@ -48,15 +48,17 @@ struct NRPlanHost {
     // arow_ptr[nb+1], arow (a_slot, col_node) pairs
     std::vector<int> arow_ptr, arow;
     std::vector<int> slot_a;  // A index of each slot, -1 for fill-only slots
+    std::vector<int> a_slots;  // slot of each A block (inverse of slot_a)
     int n_a = 0;
     // numeric factorisation schedule
-    //   level h, phase A: targets [fa_ptr[h], fa_ptr[h+1]) = (slot, pair_begin, pair_end, is_diag)
+    //   level h, phase A: targets [fa_ptr[h], fa_ptr[h+1]) = (slot, pair_begin, pair_end, flags)
+    //     flags bit 0: diagonal slot (inverted); bit 1: slot holds a Jacobian value
     //   level h, phase B: scale   [fb_ptr[h], fb_ptr[h+1]) = (L slot, D slot)
     std::vector<int> fa_ptr, targets, fb_ptr, scale;
     std::vector<int> pairs;  // (left slot, right slot)
     int64_t n_pairs = 0;
     // dense tail: the last n_tail nodes (ns = nb - n_tail sparse nodes before them);
-    // schur[4*t..] = (slot, pair_begin, pair_end, block position r*n_tail + c)
+    // schur[4*t..] = (slot, pair_begin, pair_end, block position r*n_tail + c | hasval << 30)
     int n_tail = 0, ns = 0;
     std::vector<int> schur;
     // forward solve row lists: for node k, (L slot, node m) pairs over sparse m, k in struct(m)

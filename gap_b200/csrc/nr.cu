@@ -71,7 +71,7 @@ struct gapk_nr_plan_s {
     bool uploaded = false;
     int device = -1;
     DevBuf d_yrp, d_ycol, d_bt, d_nob, d_si, d_ss, d_sa, d_lp, d_ln, d_fa, d_tg, d_pr, d_fb,
-        d_sc, d_lptr, d_lidx, d_rptr, d_rl, d_arp, d_ar, d_var, d_eq, d_schur;
+        d_sc, d_lptr, d_lidx, d_rptr, d_rl, d_arp, d_ar, d_var, d_eq, d_schur, d_aslots;
     PlanDev dev{};
 
     int upload() {
@@ -103,6 +103,7 @@ struct gapk_nr_plan_s {
         up(d_var, h.var_of_comp);
         up(d_eq, h.eq_of_comp);
         up(d_schur, h.schur);
+        up(d_aslots, h.a_slots);
         if (rc) return rc;
         cudaGetDevice(&device);
         dev.n_bus = h.n_bus;
@@ -117,6 +118,7 @@ struct gapk_nr_plan_s {
         dev.n_tail = h.n_tail;
         dev.n_schur = static_cast<int>(h.schur.size() / 4);
         dev.schur = d_schur.as<int4>();
+        dev.a_slots = d_aslots.as<int>();
         dev.y_row_ptr = d_yrp.as<int>();
         dev.y_col = d_ycol.as<int>();
         dev.bus_type = d_bt.as<int>();
@@ -197,7 +199,7 @@ void launch_body(gapk_nr_batch b, cudaStream_t st, int use_cond, cudaGraphCondit
     dim3 gm(blocks_for((long)P.n_bus * SW, 256), G);
     k_mismatch<SW><<<gm, 256, 0, st>>>(P, B);
     k_check<SW><<<1, 1024, 0, st>>>(B, use_cond, h);
-    dim3 gj(blocks_for((long)P.n_slots * SW, 256), G);
+    dim3 gj(blocks_for((long)P.n_a * SW, 256), G);
     k_jfill<T, SW><<<gj, 256, 0, st>>>(P, B);
     launch_factor<T, SW>(b, st);
     launch_solve<T, SW>(b, st, B.rhs, B.dx, 0);
@@ -282,7 +284,7 @@ struct StageOp {
                 break;
             }
             case 1: {
-                dim3 gj(blocks_for((long)P.n_slots * SW, 256), G);
+                dim3 gj(blocks_for((long)P.n_a * SW, 256), G);
                 k_jfill<T, SW><<<gj, 256, 0, st>>>(P, B);
                 break;
             }
@@ -313,7 +315,7 @@ struct KernelOp {
         const int G = b->G;
         switch (which) {
             case 0: k_mismatch<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B); break;
-            case 1: k_jfill<T, SW><<<dim3(blocks_for((long)P.n_slots * SW, 256), G), 256, 0, st>>>(P, B); break;
+            case 1: k_jfill<T, SW><<<dim3(blocks_for((long)P.n_a * SW, 256), G), 256, 0, st>>>(P, B); break;
             case 2: k_factor<T, SW><<<G, b->threads, 0, st>>>(P, B); break;
             case 3:
                 if (P.n_tail > 0)
@@ -618,6 +620,12 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
                             : cudaFuncSetAttribute(k_dense_lu<float>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)b->dense_smem);
+        if (e == cudaSuccess)
+            e = b->precision == GAPK_PREC_FP64
+                    ? cudaFuncSetAttribute(k_dense_lu<double>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout, 100)
+                    : cudaFuncSetAttribute(k_dense_lu<float>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) {
             set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
             return GAPK_ECUDA;
@@ -843,7 +851,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
                                        &h.slot_info, &h.slot_src, &h.slot_a, &h.level_ptr,
                                        &h.level_nodes, &h.fa_ptr, &h.targets, &h.pairs,
                                        &h.fb_ptr, &h.scale, &h.lptr, &h.lidx, &h.rptr,
-                                       &h.rlist, &h.arow_ptr, &h.arow, &h.schur};
+                                       &h.rlist, &h.arow_ptr, &h.arow, &h.schur, &h.a_slots};
     constexpr int kLists = sizeof(lists) / sizeof(lists[0]);
     Carver c;
     size_t loff[kLists];
@@ -921,6 +929,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
     P.arow_ptr = L(18);
     P.arow = reinterpret_cast<const int2*>(L(19));
     P.schur = reinterpret_cast<const int4*>(L(20));
+    P.a_slots = L(21);
     BatchDev D{};
     D.n_scen = 1;
     D.n_groups = 1;
@@ -963,7 +972,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
     for (int it = 0; it < in->max_iterations; ++it) {
         k_mismatch<1><<<blocks_for((long)n, 256), 256, 0, st>>>(P, D);
         k_check<1><<<1, 1024, 0, st>>>(D, 0, cudaGraphConditionalHandle{});
-        k_jfill<double, 1><<<blocks_for((long)h.n_slots, 256), 256, 0, st>>>(P, D);
+        k_jfill<double, 1><<<blocks_for((long)h.n_a, 256), 256, 0, st>>>(P, D);
         k_factor<double, 1><<<1, thr, 0, st>>>(P, D);
         if (h.n_tail > 0) {
             k_schur<double, 1><<<blocks_for((long)P.n_schur, 256), 256, 0, st>>>(P, D);

@@ -25,7 +25,8 @@ struct PlanDev {
     int n_bus, nb, nnz_y, n_slots, nnz_l, n_levels, n_a;
     int jac_mode;  // 0: reference (last duplicate, |x| <= 1e-12 dropped), 1: exact
     int ns, n_tail, n_schur;  // sparse nodes, dense-tail nodes, Schur targets (= n_tail^2)
-    const int4* schur;        // (slot, pair_begin, pair_end, block position r*n_tail + c)
+    const int4* schur;        // (slot, pair_begin, pair_end, position r*n_tail+c | hasval<<30)
+    const int* a_slots;       // slots holding Jacobian values (the only ones the fill writes)
     const int* y_row_ptr;
     const int* y_col;
     const int* bus_type;
@@ -264,8 +265,9 @@ __global__ void __launch_bounds__(256) k_jfill(PlanDev P, BatchDev B) {
     const int g = blockIdx.y;
     if (!B.gsolve[g]) return;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int slot = tid / SW, lane = tid % SW;
-    if (slot >= P.n_slots) return;
+    const int a_idx = tid / SW, lane = tid % SW;
+    if (a_idx >= P.n_a) return;
+    const int slot = P.a_slots[a_idx];
     const int4 si = P.slot_info[slot];
     const int n = P.n_bus;
     Blk<double> J = {0.0, 0.0, 0.0, 0.0};
@@ -326,12 +328,9 @@ __global__ void __launch_bounds__(256) k_jfill(PlanDev P, BatchDev B) {
     Blk<T>* F = reinterpret_cast<Blk<T>*>(B.F) + ((size_t)g * P.n_slots + slot) * SW + lane;
     stb(F, Blk<T>{(T)J.a, (T)J.b, (T)J.c, (T)J.d});
     if (B.A64) {
-        const int a = P.slot_a[slot];
-        if (a >= 0) {
-            Blk<double>* A = reinterpret_cast<Blk<double>*>(B.A64) +
-                             ((size_t)g * P.n_a + a) * SW + lane;
-            stb(A, J);
-        }
+        Blk<double>* A = reinterpret_cast<Blk<double>*>(B.A64) +
+                         ((size_t)g * P.n_a + a_idx) * SW + lane;
+        stb(A, J);
     }
 }
 
@@ -350,12 +349,12 @@ __global__ void k_factor(PlanDev P, BatchDev B) {
         const int ta = P.fa_ptr[h], tb = P.fa_ptr[h + 1];
         for (int t = ta + e0; t < tb; t += ne) {
             const int4 tg = P.targets[t];
-            Blk<T> acc = ldb(F + (size_t)tg.x * SW + lane);
+            Blk<T> acc = (tg.w & 2) ? ldb(F + (size_t)tg.x * SW + lane) : Blk<T>{0, 0, 0, 0};
             for (int p = tg.y; p < tg.z; ++p) {
                 const int2 pr = P.pairs[p];
                 msub(acc, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
             }
-            if (tg.w) {
+            if (tg.w & 1) {
                 bool ok;
                 acc = inv2(acc, ok);
                 bad |= !ok;
@@ -414,13 +413,14 @@ __global__ void __launch_bounds__(256) k_schur(PlanDev P, BatchDev B) {
     const int q = g * SW + lane;
     const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
     const int4 tg = P.schur[t];
-    Blk<T> acc = ldb(F + (size_t)tg.x * SW + lane);
+    Blk<T> acc = (tg.w >> 30) ? ldb(F + (size_t)tg.x * SW + lane) : Blk<T>{0, 0, 0, 0};
     for (int p = tg.y; p < tg.z; ++p) {
         const int2 pr = P.pairs[p];
         msub(acc, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
     }
     const int N = 2 * P.n_tail, ld = dense_ld(N);
-    const int r = 2 * (tg.w / P.n_tail), c = 2 * (tg.w % P.n_tail);
+    const int pos = tg.w & ((1 << 30) - 1);
+    const int r = 2 * (pos / P.n_tail), c = 2 * (pos % P.n_tail);
     T* D = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
     D[(size_t)r * ld + c] = acc.a;
     D[(size_t)r * ld + c + 1] = acc.b;
@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(256) k_schur(PlanDev P, BatchDev B) {
 // A pivot below 1e-14 in magnitude (the reference LU's tolerance) marks the scenario
 // singular.  Shared memory: 2 * W * dense_ld(N) elements.
 template <typename T>
-__global__ void __launch_bounds__(256) k_dense_lu(BatchDev B, int N, int W) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) k_dense_lu(BatchDev B, int N, int W) {
     const int q = blockIdx.x;
     if (q >= B.n_scen || !B.solving[q]) return;
     const int ld = dense_ld(N);
@@ -478,21 +478,14 @@ __global__ void __launch_bounds__(256) k_dense_lu(BatchDev B, int N, int W) {
             // U12 = L11^-1 A12, one column per thread; pad columns of U12 to a multiple of 8
             const int n2p = (n2 + 7) & ~7;
             for (int c = tid; c < n2p; c += nt) {
-                T x[16];
-#pragma unroll
-                for (int r = 0; r < 16; ++r) {
-                    if (r < w) {
-                        T v = T(0);
-                        if (c < n2) {
-                            v = A[(size_t)(k0 + r) * ld + k0 + w + c];
-#pragma unroll
-                            for (int qq = 0; qq < 16; ++qq)
-                                if (qq < r) v = fma(-PT[qq * ld + r], x[qq], v);
-                            A[(size_t)(k0 + r) * ld + k0 + w + c] = v;
-                        }
-                        x[r] = v;
-                        U[r * ld + c] = v;
+                for (int r = 0; r < w; ++r) {
+                    T v = T(0);
+                    if (c < n2) {
+                        v = A[(size_t)(k0 + r) * ld + k0 + w + c];
+                        for (int qq = 0; qq < r; ++qq) v = fma(-PT[qq * ld + r], U[qq * ld + c], v);
+                        A[(size_t)(k0 + r) * ld + k0 + w + c] = v;
                     }
+                    U[r * ld + c] = v;
                 }
             }
             __syncthreads();

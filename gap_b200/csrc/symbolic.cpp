@@ -317,6 +317,10 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
         P.n_a = na;
     }
     P.slot_a = slot_a;
+    // slots that carry Jacobian values, in A order (the fill kernel writes only these)
+    P.a_slots.assign(P.n_a, 0);
+    for (int sl = 0; sl < P.n_slots; ++sl)
+        if (slot_a[sl] >= 0) P.a_slots[slot_a[sl]] = sl;
     P.scale.clear();
 
     // ---- numeric factorisation schedule (left-looking block Crout) ----
@@ -401,7 +405,9 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
             P.targets.push_back(s);
             P.targets.push_back(pe.first);
             P.targets.push_back(pe.second);
-            P.targets.push_back(s < nb ? 1 : 0);
+            // bit 0: diagonal (invert); bit 1: the slot holds a Jacobian value (else it
+            // starts from zero and is never written by the fill kernel)
+            P.targets.push_back((s < nb ? 1 : 0) | (slot_a[s] >= 0 ? 2 : 0));
         }
         P.fa_ptr[h + 1] = static_cast<int>(P.targets.size() / 4);
         for (int t = P.level_ptr[h]; t < P.level_ptr[h + 1]; ++t) {
@@ -417,13 +423,16 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
     P.schur.clear();
     for (int k = ns; k < nb; ++k) {
         auto pe = emit(k);
-        P.schur.insert(P.schur.end(), {k, pe.first, pe.second, (k - ns) * T + (k - ns)});
+        auto hs = [&](int sl) { return slot_a[sl] >= 0 ? (1 << 30) : 0; };
+        P.schur.insert(P.schur.end(), {k, pe.first, pe.second, ((k - ns) * T + (k - ns)) | hs(k)});
         for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
             int a = P.lidx[p];
             pe = emit(Ubase + p);
-            P.schur.insert(P.schur.end(), {Ubase + p, pe.first, pe.second, (k - ns) * T + (a - ns)});
+            P.schur.insert(P.schur.end(), {Ubase + p, pe.first, pe.second,
+                                           ((k - ns) * T + (a - ns)) | hs(Ubase + p)});
             pe = emit(Lbase + p);
-            P.schur.insert(P.schur.end(), {Lbase + p, pe.first, pe.second, (a - ns) * T + (k - ns)});
+            P.schur.insert(P.schur.end(), {Lbase + p, pe.first, pe.second,
+                                           ((a - ns) * T + (k - ns)) | hs(Lbase + p)});
         }
     }
 

@@ -53,7 +53,7 @@ def factor(plan, F):
             acc = F[slot].copy()
             for p in range(pb, pe):
                 acc -= F[pr[p, 0]] @ F[pr[p, 1]]
-            if isd:
+            if isd & 1:
                 acc = np.linalg.inv(acc)
             F[slot] = acc
         for t in range(fb[h], fb[h + 1]):
@@ -66,7 +66,7 @@ def factor(plan, F):
         acc = F[slot].copy()
         for p in range(pb, pe):
             acc -= F[pr[p, 0]] @ F[pr[p, 1]]
-        r, c = divmod(pos, T)
+        r, c = divmod(pos & ((1 << 30) - 1), T)
         D[2 * r:2 * r + 2, 2 * c:2 * c + 2] = acc
     n = 2 * T
     for j in range(n):
