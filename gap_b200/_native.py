@@ -25,7 +25,7 @@ SCEN_CONVERGED, SCEN_MAXITER, SCEN_SINGULAR, SCEN_NONFINITE = 0, 1, 2, 3
 EXPORTS = [
     "gapk_last_error", "gapk_version", "gapk_device_count",
     "gapk_ybus_create", "gapk_ybus_destroy", "gapk_ybus_nnz", "gapk_ybus_pattern",
-    "gapk_ybus_assemble",
+    "gapk_ybus_assemble", "gapk_ybus_apply_changes",
     "gapk_nr_plan_create", "gapk_nr_plan_destroy", "gapk_nr_plan_get_info",
     "gapk_nr_plan_export",
     "gapk_nr_batch_create", "gapk_nr_batch_destroy", "gapk_nr_batch_device_bytes",
@@ -33,6 +33,8 @@ EXPORTS = [
     "gapk_nr_stage_load", "gapk_nr_stage_mismatch", "gapk_nr_stage_jacobian",
     "gapk_nr_stage_factor", "gapk_nr_stage_solve", "gapk_nr_stage_get_correction",
     "gapk_nr_stage_get_mismatch", "gapk_nr_stage_kernel", "gapk_nr_solve_noalloc",
+    "gapk_splu_create", "gapk_splu_destroy", "gapk_splu_size", "gapk_splu_factorize",
+    "gapk_splu_solve",
 ]
 
 

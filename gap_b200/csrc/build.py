@@ -74,7 +74,31 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
+    build_plugins(so, verbose=verbose, force=force)
     return so
+
+
+PLUGINS = {"libgap_admittance_gpu.so": "admittance_gpu.cpp", "libgap_lu_gpu.so": "lu_gpu.cpp",
+           "libgap_powerflow_gpu.so": "powerflow_gpu.cpp"}
+
+
+def build_plugins(core_so, verbose=False, force=False):
+    """The reference-ABI plugin libraries (dlopen'ed by name by the reference's
+    BackendFactory), linked against libgapk.so with an $ORIGIN rpath."""
+    nvcc = _nvcc()
+    pdir = os.path.join(HERE, "plugins")
+    deps = [os.path.join(pdir, "common.hpp"), os.path.join(INCLUDE, "gap_b200", "gap_interfaces.hpp"),
+            os.path.join(INCLUDE, "gapk.h"), core_so]
+    for lib, src in PLUGINS.items():
+        s = os.path.join(pdir, src)
+        out = os.path.join(LIB, lib)
+        if force or _stale(out, [s] + deps):
+            cmd = [nvcc] + ARCH + ["-x", "c++", "-std=c++20", "-O2", "-Xcompiler", "-fPIC",
+                                   "-I" + INCLUDE, "-shared", "-cudart", "static", "-o", out, s,
+                                   "-L" + LIB, "-lgapk", "-Xlinker", "-rpath=$ORIGIN"]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
 
 
 if __name__ == "__main__":

@@ -72,4 +72,11 @@ struct NRPlanHost {
 bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx,
                 const int* bus_type, int jac_mode, int ordering, int dense_min, NRPlanHost& out);
 
+// General square sparse matrix (complex values handled as 2x2 real blocks by the caller):
+// a zero-free-diagonal row permutation rp, then the same analysis as the Newton plan on the
+// permuted pattern (every position an unknown, duplicate entries summed).  val_map[e] maps
+// entry e of the permuted CSR (the plan's "Y") back to the caller's entry index.
+bool analyze_general(int n, int nnz, const int* row_ptr, const int* col_idx, int dense_min,
+                     NRPlanHost& P, std::vector<int>& rp, std::vector<int>& val_map);
+
 }  // namespace gapk

@@ -779,6 +779,152 @@ int gapk_nr_stage_get_mismatch(gapk_nr_batch b, double* d_f, void* stream) {
 }  // extern "C"
 
 // ===========================================================================================
+// General sparse LU (ILUSolver): complex a + jb handled as the 2x2 real block [a -b; b a], so
+// the Newton engine's analysis, level-scheduled factor, dense tail and solves are reused.
+// ===========================================================================================
+namespace gapk {
+
+__global__ void k_cfill(PlanDev P, BatchDev B, const double2* __restrict__ vals,
+                        const int* __restrict__ val_map) {
+    const int a_idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a_idx >= P.n_a) return;
+    const int slot = P.a_slots[a_idx];
+    const int4 si = P.slot_info[slot];
+    double re = 0.0, im = 0.0;
+    for (int e = si.z; e < si.w; ++e) {
+        const double2 v = vals[val_map[P.slot_src[e]]];
+        re += v.x;
+        im += v.y;
+    }
+    stb(reinterpret_cast<Blk<double>*>(B.F) + slot, Blk<double>{re, -im, im, re});
+}
+
+__global__ void k_crhs(int nb, const int* __restrict__ bus_of_node, const int* __restrict__ rp,
+                       const double2* __restrict__ b, double2* rhs) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nb) rhs[k] = b[rp[bus_of_node[k]]];
+}
+
+__global__ void k_csol(int nb, const int* __restrict__ bus_of_node, const double2* __restrict__ x,
+                       double2* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nb) out[bus_of_node[k]] = x[k];
+}
+
+}  // namespace gapk
+
+struct gapk_splu_s {
+    gapk_nr_plan_s plan;
+    std::vector<int> rp, val_map;
+    gapk_nr_batch batch = nullptr;
+    DevBuf d_valmap, d_rp, d_bon;
+    bool factorized = false;
+    ~gapk_splu_s() {
+        if (batch) gapk_nr_batch_destroy(batch);
+    }
+    int ready() {
+        if (batch) return GAPK_OK;
+        gapk_nr_batch_options o{GAPK_PREC_FP64, 1, 1, 512, 0};
+        int rc = gapk_nr_batch_create(&plan, 1, &o, &batch);
+        if (rc) return rc;
+        rc = d_valmap.upload(val_map);
+        if (!rc) rc = d_rp.upload(rp);
+        if (!rc) rc = d_bon.upload(plan.h.bus_of_node);
+        return rc;
+    }
+};
+
+extern "C" {
+
+int gapk_splu_create(int n, int nnz, const int* h_row_ptr, const int* h_col_idx,
+                     gapk_splu* out) {
+    if (!out || !h_row_ptr || (nnz > 0 && !h_col_idx)) {
+        set_error("gapk_splu_create: bad arguments");
+        return GAPK_EINVAL;
+    }
+    auto s = std::make_unique<gapk_splu_s>();
+    try {
+        if (!analyze_general(n, nnz, h_row_ptr, h_col_idx, 16, s->plan.h, s->rp, s->val_map))
+            return GAPK_EINVAL;
+    } catch (std::bad_alloc const&) {
+        set_error("gapk_splu_create: host allocation failed");
+        return GAPK_ENOMEM;
+    }
+    // the plan's "Y" pattern is the row-permuted matrix
+    s->plan.y_row_ptr.assign(n + 1, 0);
+    s->plan.y_col.clear();
+    for (int i = 0; i < n; ++i) {
+        const int r = s->rp[i];
+        for (int p = h_row_ptr[r]; p < h_row_ptr[r + 1]; ++p) s->plan.y_col.push_back(h_col_idx[p]);
+        s->plan.y_row_ptr[i + 1] = static_cast<int>(s->plan.y_col.size());
+    }
+    *out = s.release();
+    return GAPK_OK;
+}
+
+int gapk_splu_destroy(gapk_splu s) {
+    delete s;
+    return GAPK_OK;
+}
+
+int gapk_splu_factorize(gapk_splu s, const double* d_values, void* stream) {
+    if (!s || !d_values) {
+        set_error("gapk_splu_factorize: bad arguments");
+        return GAPK_EINVAL;
+    }
+    s->factorized = false;
+    int rc = s->ready();
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    gapk_nr_batch b = s->batch;
+    const int one[2] = {1, 0};
+    GAPK_CUDA_TRY(cudaMemcpyAsync(b->dev.gsolve, one, sizeof(int), cudaMemcpyHostToDevice, st));
+    GAPK_CUDA_TRY(cudaMemcpyAsync(b->dev.solving, one, sizeof(int), cudaMemcpyHostToDevice, st));
+    GAPK_CUDA_TRY(cudaMemcpyAsync(b->dev.singular, one + 1, sizeof(int), cudaMemcpyHostToDevice, st));
+    PlanDev const& P = s->plan.dev;
+    k_cfill<<<blocks_for((long)P.n_a, 256), 256, 0, st>>>(
+        P, b->dev, reinterpret_cast<const double2*>(d_values), s->d_valmap.as<int>());
+    launch_factor<double, 1>(b, st);
+    rc = check_launch();
+    if (rc) return rc;
+    int sing = 0;
+    GAPK_CUDA_TRY(cudaMemcpyAsync(&sing, b->dev.singular, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GAPK_CUDA_TRY(cudaStreamSynchronize(st));
+    if (sing) {
+        set_error("gapk_splu_factorize: pivot below 1e-14 (numerically singular under static "
+                  "pivoting)");
+        return GAPK_ESINGULAR;
+    }
+    s->factorized = true;
+    return GAPK_OK;
+}
+
+int gapk_splu_solve(gapk_splu s, const double* d_rhs, double* d_x, void* stream) {
+    if (!s || !d_rhs || !d_x) {
+        set_error("gapk_splu_solve: bad arguments");
+        return GAPK_EINVAL;
+    }
+    if (!s->factorized) {
+        set_error("gapk_splu_solve: matrix not factorized");
+        return GAPK_ESTATE;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    gapk_nr_batch b = s->batch;
+    const int nb = s->plan.h.nb;
+    k_crhs<<<blocks_for(nb, 256), 256, 0, st>>>(nb, s->d_bon.as<int>(), s->d_rp.as<int>(),
+                                                  reinterpret_cast<const double2*>(d_rhs),
+                                                  b->dev.rhs);
+    launch_solve<double, 1>(b, st, b->dev.rhs, b->dev.dx, 0);
+    k_csol<<<blocks_for(nb, 256), 256, 0, st>>>(nb, s->d_bon.as<int>(), b->dev.dx,
+                                                  reinterpret_cast<double2*>(d_x));
+    return check_launch();
+}
+
+int gapk_splu_size(gapk_splu s) { return s ? s->plan.h.nb : GAPK_EINVAL; }
+
+}  // extern "C"
+
+// ===========================================================================================
 // Allocation-free single-scenario solve.
 //
 // Some callers cannot call cudaMalloc at solve time: code that runs while another library

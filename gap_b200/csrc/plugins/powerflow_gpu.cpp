@@ -1,0 +1,172 @@
+// libgap_powerflow_gpu.so -- IPowerFlowSolver on the B200 Newton-Raphson engine.
+//
+// Replaces src/solver/powerflow/gpu/gpu_newton_raphson.cu (factory at :631-637) with the
+// semantics of the reference CPU solver (src/solver/powerflow/cpu/cpu_newton_raphson.cpp:
+// 33-240): per unit on buses[0].u_rated and config.base_power, specified power from the buses
+// and their in-service SOURCE/LOADGEN appliances, flat start (SLACK/PV at u_pu, PQ at 0.98),
+// the damped and clamped polar update, convergence on max |mismatch| < tolerance.  The whole
+// loop runs on the device; the plan (ordering, symbolic factorisation) is cached per Y pattern
+// and bus-type vector and rebuilt when either changes.  config.acceleration_factor is ignored,
+// as by the reference CPU solver.  set_lu_solver() is accepted but the device engine always
+// factorises with its own block LU.
+#include <cmath>
+#include <unordered_map>
+
+#include "common.hpp"
+
+namespace gapb200 {
+
+class B200NewtonRaphson final : public gap::solver::IPowerFlowSolver {
+  public:
+    ~B200NewtonRaphson() override { reset(); }
+
+    gap::solver::PowerFlowResult solve_power_flow(gap::NetworkData const& net,
+                                                  gap::SparseMatrix const& Y,
+                                                  gap::solver::PowerFlowConfig const& cfg) override {
+        gap::solver::PowerFlowResult res;
+        const int n = static_cast<int>(net.buses.size());
+        res.bus_voltages.assign(n, gap::Complex(0.0, 0.0));
+        if (n == 0 || cfg.max_iterations <= 0) {
+            res.converged = n == 0 && cfg.max_iterations > 0;
+            res.iterations = cfg.max_iterations > 0 ? 1 : 0;
+            return res;
+        }
+        if (Y.num_rows != n || static_cast<int>(Y.row_ptr.size()) != n + 1)
+            throw std::runtime_error("admittance matrix does not match the network");
+        ensure_plan(net, Y);
+        const double vb = net.buses[0].u_rated;
+        const double zb = (vb * vb) / cfg.base_power;
+        std::vector<gap::Complex> ypu(Y.nnz);
+        for (int i = 0; i < Y.nnz; ++i) ypu[i] = Y.values[i] * zb;
+        auto s = specified_power(net, cfg.base_power);
+        std::vector<double> upu(n);
+        for (int i = 0; i < n; ++i) upu[i] = net.buses[i].u_pu;
+        gapk_nr_inputs in{};
+        in.d_y = reinterpret_cast<const double*>(d_y_.upload(ypu));
+        in.d_s_spec = reinterpret_cast<const double*>(d_s_.upload(s));
+        in.d_u_pu = d_u_.upload(upu);
+        if (!cfg.use_flat_start) {
+            // the reference never initialises V without a flat start: it stays zero
+            in.d_v_init = reinterpret_cast<const double*>(d_v_.upload(res.bus_voltages));
+        }
+        in.tolerance = cfg.tolerance;
+        in.max_iterations = cfg.max_iterations;
+        in.policy = GAPK_POLICY_REFERENCE;
+        in.refine = 0;
+        gapk_nr_outputs out{};
+        out.d_v = static_cast<double*>(d_vo_.ensure(static_cast<size_t>(n) * 16));
+        out.d_iterations = static_cast<int*>(d_it_.ensure(4));
+        out.d_status = static_cast<int*>(d_st_.ensure(4));
+        out.d_final_mismatch = static_cast<double*>(d_fm_.ensure(8));
+        check(gapk_nr_solve(batch_, &in, &out, nullptr), "gapk_nr_solve");
+        check_cuda(cudaMemcpy(res.bus_voltages.data(), out.d_v, static_cast<size_t>(n) * 16,
+                              cudaMemcpyDeviceToHost),
+                   "cudaMemcpy D2H");
+        int it = 0, st = 0;
+        double fm = 0.0;
+        check_cuda(cudaMemcpy(&it, out.d_iterations, 4, cudaMemcpyDeviceToHost), "D2H");
+        check_cuda(cudaMemcpy(&st, out.d_status, 4, cudaMemcpyDeviceToHost), "D2H");
+        check_cuda(cudaMemcpy(&fm, out.d_final_mismatch, 8, cudaMemcpyDeviceToHost), "D2H");
+        res.converged = st == GAPK_SCEN_CONVERGED;
+        res.iterations = it;
+        res.final_mismatch = fm;
+        return res;
+    }
+
+    void set_lu_solver(std::shared_ptr<gap::solver::ILUSolver> lu) override { lu_ = std::move(lu); }
+
+    // Reference public method (cpu_newton_raphson.cpp:225-240): mismatches in the reference's
+    // equation order, computed with the admittance matrix as given and a fixed 100 MVA base,
+    // returned in W / var.
+    std::vector<gap::Float> calculate_mismatches(gap::NetworkData const& net,
+                                                 gap::ComplexVector const& V,
+                                                 gap::SparseMatrix const& Y) override {
+        const int n = static_cast<int>(net.buses.size());
+        if (n == 0) return {};
+        ensure_plan(net, Y);
+        const double base = 100e6;
+        auto s = specified_power(net, base);
+        gapk_nr_inputs in{};
+        in.d_y = reinterpret_cast<const double*>(d_y_.upload(Y.values));
+        in.d_s_spec = reinterpret_cast<const double*>(d_s_.upload(s));
+        in.d_v_init = reinterpret_cast<const double*>(d_v_.upload(V));
+        in.max_iterations = 1;
+        in.policy = GAPK_POLICY_NEWTON;
+        check(gapk_nr_stage_load(batch_, &in, nullptr), "gapk_nr_stage_load");
+        check(gapk_nr_stage_mismatch(batch_, nullptr), "gapk_nr_stage_mismatch");
+        gapk_nr_plan_info info{};
+        gapk_nr_plan_get_info(plan_, &info);
+        double* df = static_cast<double*>(d_f_.ensure(static_cast<size_t>(info.n_vars) * 8 + 8));
+        check(gapk_nr_stage_get_mismatch(batch_, df, nullptr), "gapk_nr_stage_get_mismatch");
+        std::vector<double> f;
+        d_f_.download(f, info.n_vars);
+        for (auto& x : f) x *= base;
+        return f;
+    }
+
+    gap::BackendType get_backend_type() const noexcept override {
+        return gap::BackendType::GPU_CUDA;
+    }
+
+  private:
+    // get_specified_power_at_bus (cpu_newton_raphson.cpp:346-377), per unit of `base`
+    static std::vector<gap::Complex> specified_power(gap::NetworkData const& net, double base) {
+        const int n = static_cast<int>(net.buses.size());
+        std::vector<gap::Complex> s(n);
+        std::unordered_map<int, std::vector<int>> by_id;
+        for (int i = 0; i < n; ++i) {
+            s[i] = gap::Complex(net.buses[i].active_power, net.buses[i].reactive_power);
+            by_id[net.buses[i].id].push_back(i);
+        }
+        for (auto const& a : net.appliances) {
+            if (a.status != 1) continue;
+            if (a.type != gap::ApplianceType::SOURCE && a.type != gap::ApplianceType::LOADGEN)
+                continue;
+            auto it = by_id.find(a.node);
+            if (it == by_id.end()) continue;
+            for (int i : it->second) s[i] += gap::Complex(a.p_specified, a.q_specified);
+        }
+        if (base > 0.0)
+            for (auto& x : s) x /= base;
+        return s;
+    }
+
+    void ensure_plan(gap::NetworkData const& net, gap::SparseMatrix const& Y) {
+        const int n = static_cast<int>(net.buses.size());
+        std::vector<int> bt(n);
+        for (int i = 0; i < n; ++i) bt[i] = static_cast<int>(net.buses[i].bus_type);
+        std::vector<int> ci(Y.col_idx.begin(), Y.col_idx.begin() + Y.nnz);
+        if (plan_ && bt == bt_ && Y.row_ptr == rp_ && ci == ci_) return;
+        reset();
+        gapk_nr_plan_options po{GAPK_JAC_REFERENCE, GAPK_ORDER_MINDEG, 0};
+        check(gapk_nr_plan_create(n, Y.nnz, Y.row_ptr.data(), ci.data(), bt.data(), &po, &plan_),
+              "gapk_nr_plan_create");
+        gapk_nr_batch_options bo{GAPK_PREC_FP64, 1, 1, 0, 1};
+        check(gapk_nr_batch_create(plan_, 1, &bo, &batch_), "gapk_nr_batch_create");
+        bt_ = bt;
+        rp_ = Y.row_ptr;
+        ci_ = ci;
+    }
+
+    void reset() {
+        if (batch_) gapk_nr_batch_destroy(batch_);
+        if (plan_) gapk_nr_plan_destroy(plan_);
+        batch_ = nullptr;
+        plan_ = nullptr;
+    }
+
+    std::shared_ptr<gap::solver::ILUSolver> lu_;
+    gapk_nr_plan plan_ = nullptr;
+    gapk_nr_batch batch_ = nullptr;
+    std::vector<int> bt_, rp_, ci_;
+    DeviceBuffer d_y_, d_s_, d_u_, d_v_, d_vo_, d_it_, d_st_, d_fm_, d_f_;
+};
+
+}  // namespace gapb200
+
+extern "C" {
+gap::solver::IPowerFlowSolver* create_gpu_powerflow_solver() {
+    return new gapb200::B200NewtonRaphson();
+}
+void destroy_gpu_powerflow_solver(gap::solver::IPowerFlowSolver* instance) { delete instance; }
+}

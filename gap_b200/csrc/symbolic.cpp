@@ -482,3 +482,95 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
 }
 
 }  // namespace gapk
+
+namespace gapk {
+
+// Row permutation giving a zero-free diagonal (maximum transversal by depth-first augmenting
+// paths, Duff's MC21 method): on success rp[i] is the original row placed at position i, with
+// A[rp[i]][i] structurally non-zero.  Returns false when the pattern is structurally singular.
+static bool zero_free_diagonal(int n, const int* row_ptr, const int* col_idx,
+                               std::vector<int>& rp) {
+    std::vector<int> col_row(n, -1), row_col(n, -1), seen(n, -1);
+    std::vector<int> rows, pos, via;
+    for (int r0 = 0; r0 < n; ++r0) {
+        int found = -1;
+        for (int p = row_ptr[r0]; p < row_ptr[r0 + 1]; ++p)
+            if (col_row[col_idx[p]] < 0) {
+                found = col_idx[p];
+                break;
+            }
+        rows.assign(1, r0);
+        pos.assign(1, row_ptr[r0]);
+        via.clear();
+        // depth-first search for an augmenting path; via[d] leads from rows[d] to rows[d+1]
+        while (found < 0 && !rows.empty()) {
+            const int d = static_cast<int>(rows.size()) - 1;
+            const int u = rows[d];
+            if (pos[d] == row_ptr[u + 1]) {
+                rows.pop_back();
+                pos.pop_back();
+                if (!via.empty()) via.pop_back();
+                continue;
+            }
+            const int c = col_idx[pos[d]++];
+            if (seen[c] == r0) continue;
+            seen[c] = r0;
+            if (col_row[c] < 0) {
+                found = c;
+                break;
+            }
+            via.push_back(c);
+            rows.push_back(col_row[c]);
+            pos.push_back(row_ptr[col_row[c]]);
+        }
+        if (found < 0) return false;
+        int c = found;
+        for (int d = static_cast<int>(rows.size()) - 1; d >= 0; --d) {
+            col_row[c] = rows[d];
+            row_col[rows[d]] = c;
+            c = d > 0 ? via[d - 1] : -1;
+        }
+    }
+    rp = col_row;
+    return true;
+}
+
+bool analyze_general(int n, int nnz, const int* row_ptr, const int* col_idx, int dense_min,
+                     NRPlanHost& P, std::vector<int>& rp, std::vector<int>& val_map) {
+    if (n <= 0 || nnz <= 0 || row_ptr[0] != 0 || row_ptr[n] != nnz) {
+        set_error("matrix must be square with a consistent, non-empty CSR pattern");
+        return false;
+    }
+    for (int i = 0; i < n; ++i)
+        if (row_ptr[i + 1] < row_ptr[i]) {
+            set_error("row_ptr not monotone");
+            return false;
+        }
+    for (int p = 0; p < nnz; ++p)
+        if (col_idx[p] < 0 || col_idx[p] >= n) {
+            set_error("col_idx out of range");
+            return false;
+        }
+    if (!zero_free_diagonal(n, row_ptr, col_idx, rp)) {
+        set_error("matrix is structurally singular (no zero-free diagonal)");
+        return false;
+    }
+    // B = P A: row i of B is row rp[i] of A; val_map[e] = index in A of B's entry e
+    std::vector<int> brp(n + 1, 0), bci;
+    bci.reserve(nnz);
+    val_map.clear();
+    val_map.reserve(nnz);
+    for (int i = 0; i < n; ++i) {
+        int r = rp[i];
+        for (int p = row_ptr[r]; p < row_ptr[r + 1]; ++p) {
+            bci.push_back(col_idx[p]);
+            val_map.push_back(p);
+        }
+        brp[i + 1] = static_cast<int>(bci.size());
+    }
+    std::vector<int> bt(n, 0);  // every position is an unknown ("PQ")
+    if (!analyze_nr(n, nnz, brp.data(), bci.data(), bt.data(), 1, 0, dense_min, P)) return false;
+    return true;
+}
+
+}  // namespace gapk

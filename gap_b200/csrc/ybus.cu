@@ -100,6 +100,50 @@ __global__ void k_ybus(int nnz, int n_scen, const int* __restrict__ slot_src,
     out[(size_t)s * out_stride + p] = make_double2(vr, vi);
 }
 
+// Branch status changes applied to existing values, in change order (one thread: the deltas
+// of different changes may hit the same entry, and the reference applies them sequentially,
+// src/admittance/cpu/cpu_admittance_matrix.cpp:214-297).  pos = (diag f, diag t, (f,t), (t,f))
+// CSR indices or -1; prm = (r1, x1, g1, b1, status).
+__global__ void k_ybus_changes(int n, const int* __restrict__ pos, const double* __restrict__ prm,
+                               double2* values) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int i = 0; i < n; ++i) {
+        const double* q = prm + (size_t)i * 5;
+        const double r = q[0], x = q[1], g = q[2], b = q[3];
+        const double z2 = __dadd_rn(__dmul_rn(r, r), __dmul_rn(x, x));
+        double yr = 0.0, yi = 0.0;
+        if (z2 > 1e-12) {
+            yr = __ddiv_rn(r, z2);
+            yi = __ddiv_rn(-x, z2);
+        }
+        // total = series + (g1 + j b1); the diagonals also get j b1/2 (the reference's
+        // update adds both, unlike its build)
+        double tr = __dadd_rn(yr, g), ti = __dadd_rn(yi, b);
+        double sr = 0.0, si = __ddiv_rn(b, 2.0);
+        double orr = yr, oi = yi;
+        if (q[4] == 0.0) {
+            tr = -tr;
+            ti = -ti;
+            si = -si;
+            orr = -orr;
+            oi = -oi;
+            sr = -sr;
+        }
+        const double dr = __dadd_rn(tr, sr), di = __dadd_rn(ti, si);
+        const int* p = pos + (size_t)i * 4;
+        for (int k = 0; k < 2; ++k)
+            if (p[k] >= 0) {
+                double2 v = values[p[k]];
+                values[p[k]] = make_double2(__dadd_rn(v.x, dr), __dadd_rn(v.y, di));
+            }
+        for (int k = 2; k < 4; ++k)
+            if (p[k] >= 0) {
+                double2 v = values[p[k]];
+                values[p[k]] = make_double2(__dsub_rn(v.x, orr), __dsub_rn(v.y, oi));
+            }
+    }
+}
+
 }  // namespace
 }  // namespace gapk
 
@@ -194,6 +238,23 @@ int gapk_ybus_assemble(gapk_ybus y, int n_scen, const double* d_branch, int64_t 
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string("k_ybus launch: ") + cudaGetErrorString(e));
+        return GAPK_ECUDA;
+    }
+    return GAPK_OK;
+}
+
+int gapk_ybus_apply_changes(int n_changes, const int* d_pos, const double* d_params,
+                            double* d_values, void* stream) {
+    if (n_changes < 0 || (n_changes > 0 && (!d_pos || !d_params || !d_values))) {
+        set_error("gapk_ybus_apply_changes: bad arguments");
+        return GAPK_EINVAL;
+    }
+    if (n_changes == 0) return GAPK_OK;
+    k_ybus_changes<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(
+        n_changes, d_pos, d_params, reinterpret_cast<double2*>(d_values));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("k_ybus_changes launch: ") + cudaGetErrorString(e));
         return GAPK_ECUDA;
     }
     return GAPK_OK;

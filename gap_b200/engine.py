@@ -269,3 +269,47 @@ class NRBatch:
                 self._h = None
         except Exception:
             pass
+
+
+# ----------------------------------------------------------------------------------------
+# General sparse LU
+# ----------------------------------------------------------------------------------------
+
+
+class SparseLU:
+    """Complex square sparse LU on the device (ILUSolver, include/gap/solver/
+    lu_solver_interface.h:21-35): host analysis once per pattern, device factorisation with
+    static pivoting (after a zero-free-diagonal row matching) and device solves."""
+
+    def __init__(self, row_ptr, col_idx):
+        rp = N.i32(row_ptr)
+        ci = N.i32(col_idx)
+        h = C.c_void_p()
+        N.check(N.lib().gapk_splu_create(C.c_int(len(rp) - 1), C.c_int(len(ci)), N.iptr(rp),
+                                         N.iptr(ci), C.byref(h)))
+        self._h = h
+        self.n = int(N.lib().gapk_splu_size(h))
+
+    def factorize(self, values, stream=None) -> bool:
+        """values: complex128 [nnz] on the device.  False when a pivot is (numerically)
+        zero; other failures raise."""
+        require_cuda()
+        rc = N.lib().gapk_splu_factorize(self._h, _dptr(values), _stream_ptr(stream))
+        if rc == -5:
+            return False
+        N.check(rc)
+        return True
+
+    def solve(self, rhs, stream=None):
+        torch = _torch()
+        x = torch.empty_like(rhs)
+        N.check(N.lib().gapk_splu_solve(self._h, _dptr(rhs), _dptr(x), _stream_ptr(stream)))
+        return x
+
+    def __del__(self):
+        try:
+            if self._h:
+                N.lib().gapk_splu_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass

@@ -94,6 +94,13 @@ int gapk_ybus_assemble(gapk_ybus y, int n_scen, const double* d_branch, int64_t 
                        const double* d_shunt, int64_t shunt_stride, int mode, double scale,
                        double* d_values, int64_t values_stride, void* stream);
 
+/* Branch status changes on existing Y values (IAdmittanceMatrix::update_admittance_matrix,
+ * src/admittance/cpu/cpu_admittance_matrix.cpp:204-301), applied on the device in change
+ * order.  d_pos[i*4..] = CSR indices of (diag from, diag to, (from,to), (to,from)) or -1, as
+ * the caller located them in the pattern; d_params[i*5..] = (r1, x1, g1, b1, status). */
+int gapk_ybus_apply_changes(int n_changes, const int* d_pos, const double* d_params,
+                            double* d_values, void* stream);
+
 /* ==== Newton-Raphson engine ===========================================================
  * A plan holds everything that depends only on the Y pattern and the bus types: the
  * 2x2-block Jacobian pattern, a minimum-degree ordering, the symbolic block-LU
@@ -193,6 +200,23 @@ typedef struct {
 /* Runs the whole Newton-Raphson loop on the device.  Asynchronous on `stream`. */
 int gapk_nr_solve(gapk_nr_batch b, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
                   void* stream);
+
+/* ==== General sparse LU (ILUSolver) =====================================================
+ * Complex square CSR matrices (values interleaved re, im).  Analysis once per pattern on the
+ * host: a row permutation giving a zero-free diagonal (maximum transversal), minimum-degree
+ * ordering of the symmetrised pattern, symbolic factorisation; numeric factorisation and
+ * solves on the device with static pivoting (a pivot below 1e-14 reports GAPK_ESINGULAR,
+ * as CPULUSolver's pivot tolerance, src/solver/lu/cpu/cpu_lu_solver.cpp:65).  Duplicate
+ * entries are summed.  Replaces ILUSolver::factorize / solve / update_factorization
+ * (include/gap/solver/lu_solver_interface.h:21-35). */
+typedef struct gapk_splu_s* gapk_splu;
+int gapk_splu_create(int n, int nnz, const int* h_row_ptr, const int* h_col_idx, gapk_splu* out);
+int gapk_splu_destroy(gapk_splu s);
+int gapk_splu_size(gapk_splu s);
+/* Factorises d_values (complex [nnz], device); synchronises the stream to report the result. */
+int gapk_splu_factorize(gapk_splu s, const double* d_values, void* stream);
+/* x = A^-1 b for complex device vectors of length n. */
+int gapk_splu_solve(gapk_splu s, const double* d_rhs, double* d_x, void* stream);
 
 /* Allocation-free variant of gapk_nr_solve for ONE scenario in FP64 (no counterpart in the
  * reference).  For callers that may not allocate device memory while they solve -- code

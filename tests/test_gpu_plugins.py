@@ -1,0 +1,71 @@
+"""The drop-in boundary: the B200 plugin libraries loaded by a caller compiled against the
+reference's own headers (oracle/_ref/abi_driver, built from oracle/abi_driver.cpp) and
+compared, through the reference's interfaces, with the reference CPU backends."""
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import fixture_names, network_of
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "abi_driver")
+LIBDIR = os.path.join(ROOT, "gap_b200", "lib")
+
+
+def write_net(net, path, tol=1e-8, max_iter=20, base=1e6):
+    with open(path, "w") as f:
+        f.write(f"{net.n_bus}\n")
+        for i in range(net.n_bus):
+            f.write(f"{net.bus_id[i]} {net.u_rated[i]!r} {net.bus_type[i]} {net.u_pu[i]!r} "
+                    f"{net.p[i]!r} {net.q[i]!r}\n")
+        f.write(f"{net.n_branch}\n")
+        for b in range(net.n_branch):
+            f.write(f"{net.br_id[b]} {net.from_id[b]} {net.to_id[b]} {net.status[b]} "
+                    f"{net.r1[b]!r} {net.x1[b]!r} {net.g1[b]!r} {net.b1[b]!r} {net.k[b]!r} "
+                    f"{net.theta[b]!r}\n")
+        f.write(f"{net.n_app}\n")
+        for a in range(net.n_app):
+            f.write(f"{net.app_id[a]} {net.app_node[a]} {net.app_status[a]} {net.app_type[a]} "
+                    f"{net.app_p[a]!r} {net.app_q[a]!r} {net.app_g1[a]!r} {net.app_b1[a]!r}\n")
+        f.write(f"{tol!r} {max_iter} {base!r}\n")
+
+
+def run_driver(net, tmp_path, base):
+    p = tmp_path / "net.txt"
+    write_net(net, p, base=base)
+    r = subprocess.run([DRIVER, LIBDIR, str(p)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = {}
+    for line in r.stdout.splitlines():
+        k, *v = line.split()
+        out[k] = [float(x) for x in v]
+    return out
+
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not os.path.exists(DRIVER), reason="abi driver not built")]
+
+
+@pytest.mark.parametrize("name", [n for n in fixture_names("kat_") if n != "kat_update"]
+                         + ["c0_seed0", "c0_seed3", "pgm_radial_3feeder_8nodepf"])
+def test_plugins_drop_in_against_reference_backends(name, tmp_path):
+    net, d = network_of(name)
+    o = run_driver(net, tmp_path, float(d["base_power"]))
+    assert o["backend"] == [1, 1, 1]  # BackendType::GPU_CUDA from all three
+    assert o["ybus_pattern_equal"] == [1] and o["ybus_values_equal"] == [1]
+    assert o["update_rel_diff"][0] <= 1e-14
+    cc, cg = o["nr_converged"]
+    assert cc == cg
+    ic, ig = o["nr_iterations"]
+    assert abs(ic - ig) <= 1
+    if cc:
+        assert o["nr_max_dv"][0] < 1e-8 and o["nr_max_dangle"][0] < 1e-8
+    assert o["mismatch_sizes"][0] == o["mismatch_sizes"][1]
+    dm, sm = o["mismatch_max_abs_diff"]
+    assert dm <= 1e-9 * sm + 1e-6
+    assert o["lu_factorized"] == [1, 1, 1]
+    assert o["lu_rel_diff"][0] < 1e-10
+    assert o["lu_bad_rhs_throws"] == [1]

@@ -153,3 +153,28 @@ def test_synth_generators_deterministic():
     br = synth.bridges(a.n_bus, f, t)
     out = synth.n_minus_1(a, 20)
     assert len(out) == 20 and not br[out].any()
+
+
+def test_sparse_lu_analysis_matching_and_errors():
+    from gap_b200 import _native as N
+    from gap_b200.engine import SparseLU
+
+    # zero diagonal: [[0, 1], [1, 0]] needs the row matching
+    lu = SparseLU([0, 1, 2], [1, 0])
+    assert lu.n == 2
+    # structurally singular: both rows only in column 0
+    with pytest.raises(N.GapkError):
+        SparseLU([0, 1, 2], [0, 0])
+    # empty / non-square-like patterns are rejected (reference: factorize() returns false)
+    with pytest.raises(N.GapkError):
+        SparseLU([0, 0, 0], [])
+    rng = np.random.default_rng(4)
+    for n in (5, 40, 200):
+        A = (rng.random((n, n)) < 0.05)
+        perm = rng.permutation(n)
+        np.fill_diagonal(A, False)
+        A[perm, np.arange(n)] = True   # a transversal exists, mostly off the diagonal
+        rows, cols = np.nonzero(A)
+        rp = np.zeros(n + 1, np.int32)
+        np.add.at(rp, rows + 1, 1)
+        assert SparseLU(np.cumsum(rp), cols).n == n
