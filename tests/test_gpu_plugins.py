@@ -16,21 +16,29 @@ LIBDIR = os.path.join(ROOT, "gap_b200", "lib")
 
 
 def write_net(net, path, tol=1e-8, max_iter=20, base=1e6):
-    with open(path, "w") as f:
-        f.write(f"{net.n_bus}\n")
-        for i in range(net.n_bus):
-            f.write(f"{net.bus_id[i]} {net.u_rated[i]!r} {net.bus_type[i]} {net.u_pu[i]!r} "
-                    f"{net.p[i]!r} {net.q[i]!r}\n")
-        f.write(f"{net.n_branch}\n")
-        for b in range(net.n_branch):
-            f.write(f"{net.br_id[b]} {net.from_id[b]} {net.to_id[b]} {net.status[b]} "
-                    f"{net.r1[b]!r} {net.x1[b]!r} {net.g1[b]!r} {net.b1[b]!r} {net.k[b]!r} "
-                    f"{net.theta[b]!r}\n")
-        f.write(f"{net.n_app}\n")
-        for a in range(net.n_app):
-            f.write(f"{net.app_id[a]} {net.app_node[a]} {net.app_status[a]} {net.app_type[a]} "
-                    f"{net.app_p[a]!r} {net.app_q[a]!r} {net.app_g1[a]!r} {net.app_b1[a]!r}\n")
-        f.write(f"{tol!r} {max_iter} {base!r}\n")
+    def f(x):
+        return repr(float(x))
+
+    def i(x):
+        return str(int(x))
+
+    lines = [i(net.n_bus)]
+    for k in range(net.n_bus):
+        lines.append(" ".join([i(net.bus_id[k]), f(net.u_rated[k]), i(net.bus_type[k]),
+                               f(net.u_pu[k]), f(net.p[k]), f(net.q[k])]))
+    lines.append(i(net.n_branch))
+    for b in range(net.n_branch):
+        lines.append(" ".join([i(net.br_id[b]), i(net.from_id[b]), i(net.to_id[b]),
+                               i(net.status[b])] + [f(getattr(net, a)[b]) for a in
+                                                    ("r1", "x1", "g1", "b1", "k", "theta")]))
+    lines.append(i(net.n_app))
+    for a in range(net.n_app):
+        lines.append(" ".join([i(net.app_id[a]), i(net.app_node[a]), i(net.app_status[a]),
+                               i(net.app_type[a])] + [f(getattr(net, c)[a]) for c in
+                                                      ("app_p", "app_q", "app_g1", "app_b1")]))
+    lines.append(" ".join([f(tol), i(max_iter), f(base)]))
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
 
 
 def run_driver(net, tmp_path, base):
