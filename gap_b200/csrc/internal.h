@@ -49,6 +49,7 @@ struct NRPlanHost {
     std::vector<int> arow_ptr, arow;
     std::vector<int> slot_a;  // A index of each slot, -1 for fill-only slots
     std::vector<int> a_slots;  // slot of each A block (inverse of slot_a)
+    std::vector<int> acol_ptr, acol;  // A blocks by block column: (a index, row node) pairs
     int n_a = 0;
     // numeric factorisation schedule
     //   level h, phase A: targets [fa_ptr[h], fa_ptr[h+1]) = (slot, pair_begin, pair_end, flags)

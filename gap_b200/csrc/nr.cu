@@ -71,7 +71,7 @@ struct gapk_nr_plan_s {
     bool uploaded = false;
     int device = -1;
     DevBuf d_yrp, d_ycol, d_bt, d_nob, d_si, d_ss, d_sa, d_lp, d_ln, d_fa, d_tg, d_pr, d_fb,
-        d_sc, d_lptr, d_lidx, d_rptr, d_rl, d_arp, d_ar, d_var, d_eq, d_schur, d_aslots;
+        d_sc, d_lptr, d_lidx, d_rptr, d_rl, d_arp, d_ar, d_var, d_eq, d_schur, d_aslots, d_acp, d_ac;
     PlanDev dev{};
 
     int upload() {
@@ -104,6 +104,8 @@ struct gapk_nr_plan_s {
         up(d_eq, h.eq_of_comp);
         up(d_schur, h.schur);
         up(d_aslots, h.a_slots);
+        up(d_acp, h.acol_ptr);
+        up(d_ac, h.acol);
         if (rc) return rc;
         cudaGetDevice(&device);
         dev.n_bus = h.n_bus;
@@ -119,6 +121,8 @@ struct gapk_nr_plan_s {
         dev.n_schur = static_cast<int>(h.schur.size() / 4);
         dev.schur = d_schur.as<int4>();
         dev.a_slots = d_aslots.as<int>();
+        dev.acol_ptr = d_acp.as<int>();
+        dev.acol = d_ac.as<int2>();
         dev.y_row_ptr = d_yrp.as<int>();
         dev.y_col = d_ycol.as<int>();
         dev.bus_type = d_bt.as<int>();
@@ -335,6 +339,45 @@ struct KernelOp {
         }
     }
 };
+template <typename T, int SW>
+void launch_solve_t(gapk_nr_batch b, cudaStream_t st, const double2* rhs, double2* out, int acc) {
+    PlanDev const& P = b->plan->dev;
+    BatchDev const& B = b->dev;
+    k_solve_fwd_t<T, SW><<<b->G, b->threads, 0, st>>>(P, B, rhs);
+    if (P.n_tail > 0)
+        k_dense_solve_t<T, SW><<<b->G * SW, 256, 2 * P.n_tail * sizeof(T), st>>>(P, B, out, acc);
+    k_solve_bwd_t<T, SW><<<b->G, b->threads, 0, st>>>(P, B, out, acc);
+}
+
+template <typename T, int SW>
+struct AdjointOp {
+    static void run(gapk_nr_batch b, const double* dvm, const double* dva, double* dp, double* dq,
+                    cudaStream_t st) {
+        PlanDev const& P = b->plan->dev;
+        BatchDev const& B = b->dev;
+        const int G = b->G;
+        k_adj_prep<SW><<<blocks_for((long)G * SW, 256), 256, 0, st>>>(B);
+        k_mismatch<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B);
+        k_jfill<T, SW><<<dim3(blocks_for((long)P.n_a * SW, 256), G), 256, 0, st>>>(P, B);
+        launch_factor<T, SW>(b, st);
+        k_adj_rhs<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B, dvm, dva);
+        launch_solve_t<T, SW>(b, st, B.rhs, B.dx, 0);
+        if (B.A64) {
+            k_residual_t<SW><<<dim3(blocks_for((long)P.nb * SW, 256), G), 256, 0, st>>>(P, B);
+            launch_solve_t<T, SW>(b, st, B.res, B.dx, 1);
+        }
+        k_adj_out<SW><<<blocks_for((long)b->n_scen * P.n_bus, 256), 256, 0, st>>>(P, B, dp, dq);
+    }
+};
+template <typename T, int SW>
+struct AdjBranchOp {
+    static void run(gapk_nr_batch b, int m, const int* f, const int* t, const double* brp, double* dr,
+                    double* dx, cudaStream_t st) {
+        k_adj_branch<SW><<<blocks_for((long)b->n_scen * m, 256), 256, 0, st>>>(
+            b->plan->dev, b->dev, m, f, t, brp, dr, dx);
+    }
+};
+
 template <typename T, int SW>
 struct ToRefOp {
     static void run(gapk_nr_batch b, const double2* src, const int* map, int n_out, double sign,
@@ -759,6 +802,31 @@ int gapk_nr_stage_kernel(gapk_nr_batch b, int kernel, void* stream) {
         return GAPK_EINVAL;
     }
     dispatch_tsw<KernelOp>(b->precision, b->sw, b, kernel, static_cast<cudaStream_t>(stream));
+    return check_launch();
+}
+
+int gapk_nr_adjoint(gapk_nr_batch b, const double* d_dl_dvm, const double* d_dl_dva,
+                    double* d_dl_dp, double* d_dl_dq, void* stream) {
+    if (!b || !d_dl_dvm || !d_dl_dva) {
+        set_error("gapk_nr_adjoint: bad arguments");
+        return GAPK_EINVAL;
+    }
+    dispatch_tsw<AdjointOp>(b->precision, b->sw, b, d_dl_dvm, d_dl_dva, d_dl_dp, d_dl_dq,
+                            static_cast<cudaStream_t>(stream));
+    return check_launch();
+}
+
+int gapk_nr_adjoint_branch(gapk_nr_batch b, int n_branch, const int* d_from, const int* d_to,
+                           const double* d_branch_pu, double* d_dl_dr, double* d_dl_dx,
+                           void* stream) {
+    if (!b || n_branch < 0 || (n_branch > 0 && (!d_from || !d_to || !d_branch_pu || !d_dl_dr ||
+                                                !d_dl_dx))) {
+        set_error("gapk_nr_adjoint_branch: bad arguments");
+        return GAPK_EINVAL;
+    }
+    if (n_branch == 0) return GAPK_OK;
+    dispatch_tsw<AdjBranchOp>(b->precision, b->sw, b, n_branch, d_from, d_to, d_branch_pu,
+                              d_dl_dr, d_dl_dx, static_cast<cudaStream_t>(stream));
     return check_launch();
 }
 

@@ -27,6 +27,8 @@ struct PlanDev {
     int ns, n_tail, n_schur;  // sparse nodes, dense-tail nodes, Schur targets (= n_tail^2)
     const int4* schur;        // (slot, pair_begin, pair_end, position r*n_tail+c | hasval<<30)
     const int* a_slots;       // slots holding Jacobian values (the only ones the fill writes)
+    const int* acol_ptr;      // A blocks by block column: (a index, row node)
+    const int2* acol;
     const int* y_row_ptr;
     const int* y_col;
     const int* bus_type;
@@ -803,6 +805,281 @@ __global__ void k_node_to_ref(const double2* __restrict__ src, int nb, int n_sce
     const int a = map[2 * k], b = map[2 * k + 1];
     if (a >= 0) dst[(size_t)s * n_vars + a] = sign * v.x;
     if (b >= 0) dst[(size_t)s * n_vars + b] = sign * v.y;
+}
+
+// ---------------------------------------------------------------------------------------
+// adjoint: J^T lambda = dL/dx with the factors of J = L U
+//   U^T z = g   : sparse forward sweep with U slots transposed (D^-T on sparse nodes), the
+//                 tail gathers its sparse contributions, then a dense U_tt^T solve
+//   L^T lam = z : dense L_tt^T solve, then a sparse backward sweep with L slots transposed
+// ---------------------------------------------------------------------------------------
+template <int SW>
+__global__ void k_adj_prep(BatchDev B) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= B.n_groups * SW) return;
+    B.solving[q] = q < B.n_scen ? 1 : 0;
+    B.singular[q] = 0;
+    if (q % SW == 0) {
+        B.gsolve[q / SW] = 1;
+        B.giter[q / SW] = 1;
+    }
+}
+
+// g per node: (dL/dtheta, dL/d|V| for PQ buses); inputs scenario-major [n_scen][n_bus]
+template <int SW>
+__global__ void k_adj_rhs(PlanDev P, BatchDev B, const double* __restrict__ dvm,
+                          const double* __restrict__ dva) {
+    const int g = blockIdx.y;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = tid / SW, lane = tid % SW;
+    if (i >= P.n_bus) return;
+    const int node = P.node_of_bus[i];
+    if (node < 0) return;
+    const int q = g * SW + lane;
+    const int src = q < B.n_scen ? q : g * SW;
+    const double gt = dva[(size_t)src * P.n_bus + i];
+    const double gv = P.bus_type[i] == BUS_PQ ? dvm[(size_t)src * P.n_bus + i] : 0.0;
+    B.rhs[((size_t)g * P.nb + node) * SW + lane] = make_double2(gt, gv);
+}
+
+template <typename T, int SW>
+__global__ void k_solve_fwd_t(PlanDev P, BatchDev B, const double2* __restrict__ rhs) {
+    const int g = blockIdx.x;
+    if (!B.gsolve[g]) return;
+    const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
+    Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
+    const double2* R = rhs + (size_t)g * P.nb * SW;
+    const int lane = threadIdx.x % SW;
+    const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
+    for (int h = 0; h < P.n_levels; ++h) {
+        for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
+            const int j = P.level_nodes[t];
+            const double2 b = R[(size_t)j * SW + lane];
+            Vec2<T> acc = {(T)b.x, (T)b.y};
+            for (int q = P.rptr[j]; q < P.rptr[j + 1]; ++q) {
+                const int2 r = P.rlist[q];  // (L slot of (j,k), k); U(k,j) sits nnz_l further
+                msubtv(acc, ldb(F + (size_t)(r.x + P.nnz_l) * SW + lane),
+                       ldv(X + (size_t)r.y * SW + lane));
+            }
+            stv(X + (size_t)j * SW + lane, multv(ldb(F + (size_t)j * SW + lane), acc));
+        }
+        __syncthreads();
+    }
+    for (int j = P.ns + e0; j < P.nb; j += ne) {
+        const double2 b = R[(size_t)j * SW + lane];
+        Vec2<T> acc = {(T)b.x, (T)b.y};
+        for (int q = P.rptr[j]; q < P.rptr[j + 1]; ++q) {
+            const int2 r = P.rlist[q];
+            msubtv(acc, ldb(F + (size_t)(r.x + P.nnz_l) * SW + lane),
+                   ldv(X + (size_t)r.y * SW + lane));
+        }
+        stv(X + (size_t)j * SW + lane, acc);
+    }
+}
+
+template <typename T, int SW>
+__global__ void __launch_bounds__(256) k_dense_solve_t(PlanDev P, BatchDev B, double2* out,
+                                                       int accumulate) {
+    const int q = blockIdx.x;
+    if (q >= B.n_scen || !B.solving[q]) return;
+    const int g = q / SW, lane = q % SW;
+    const int N = 2 * P.n_tail, ld = dense_ld(N);
+    const T* A = reinterpret_cast<const T*>(B.Dt) + (size_t)q * N * ld;
+    Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* y = reinterpret_cast<T*>(smraw);
+    const int tid = threadIdx.x, wid = tid >> 5, ln = tid & 31, nw = blockDim.x >> 5;
+    for (int i = tid; i < P.n_tail; i += blockDim.x) {
+        const Vec2<T> v = ldv(X + (size_t)(P.ns + i) * SW + lane);
+        y[2 * i] = v.x;
+        y[2 * i + 1] = v.y;
+    }
+    __syncthreads();
+    // U^T w = y (lower triangular with U's diagonal)
+    for (int r0 = 0; r0 < N; r0 += 32) {
+        for (int rr = wid; rr < 32; rr += nw) {
+            const int row = r0 + rr;
+            if (row >= N) continue;
+            T acc = T(0);
+            for (int c = ln; c < r0; c += 32) acc = fma(A[(size_t)c * ld + row], y[c], acc);
+#pragma unroll
+            for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+            if (ln == 0) y[row] -= acc;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            const int row = r0 + ln;
+            T v = row < N ? y[row] : T(0);
+            for (int j = 0; j < 32; ++j) {
+                if (r0 + j >= N) break;
+                if (ln == j) v = v / A[(size_t)row * ld + row];
+                const T vj = __shfl_sync(0xffffffffu, v, j);
+                if (ln > j && row < N) v = fma(-A[(size_t)(r0 + j) * ld + row], vj, v);
+            }
+            if (row < N) y[row] = v;
+        }
+        __syncthreads();
+    }
+    // L^T lam = w (unit upper triangular)
+    const int last = ((N - 1) / 32) * 32;
+    for (int r0 = last; r0 >= 0; r0 -= 32) {
+        const int r1 = min(r0 + 32, N);
+        for (int rr = wid; rr < 32; rr += nw) {
+            const int row = r0 + rr;
+            if (row >= N) continue;
+            T acc = T(0);
+            for (int c = r1 + ln; c < N; c += 32) acc = fma(A[(size_t)c * ld + row], y[c], acc);
+#pragma unroll
+            for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+            if (ln == 0) y[row] -= acc;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            const int row = r0 + ln;
+            T v = row < N ? y[row] : T(0);
+            for (int j = 31; j >= 0; --j) {
+                if (r0 + j >= N) continue;
+                const T vj = __shfl_sync(0xffffffffu, v, j);
+                if (ln < j && row < N) v = fma(-A[(size_t)(r0 + j) * ld + row], vj, v);
+            }
+            if (row < N) y[row] = v;
+        }
+        __syncthreads();
+    }
+    double2* O = out + (size_t)g * P.nb * SW;
+    for (int i = tid; i < P.n_tail; i += blockDim.x) {
+        const int k = P.ns + i;
+        stv(X + (size_t)k * SW + lane, Vec2<T>{y[2 * i], y[2 * i + 1]});
+        double2* o = O + (size_t)k * SW + lane;
+        if (accumulate) {
+            const double2 old = *o;
+            *o = make_double2(old.x + (double)y[2 * i], old.y + (double)y[2 * i + 1]);
+        } else {
+            *o = make_double2((double)y[2 * i], (double)y[2 * i + 1]);
+        }
+    }
+}
+
+template <typename T, int SW>
+__global__ void k_solve_bwd_t(PlanDev P, BatchDev B, double2* out, int accumulate) {
+    const int g = blockIdx.x;
+    if (!B.gsolve[g]) return;
+    const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
+    Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
+    double2* O = out + (size_t)g * P.nb * SW;
+    const int lane = threadIdx.x % SW;
+    const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
+    for (int h = P.n_levels - 1; h >= 0; --h) {
+        for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
+            const int k = P.level_nodes[t];
+            Vec2<T> acc = ldv(X + (size_t)k * SW + lane);
+            for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
+                msubtv(acc, ldb(F + (size_t)(P.nb + p) * SW + lane),
+                       ldv(X + (size_t)P.lidx[p] * SW + lane));
+            }
+            stv(X + (size_t)k * SW + lane, acc);
+            double2* o = O + (size_t)k * SW + lane;
+            if (accumulate) {
+                const double2 old = *o;
+                *o = make_double2(old.x + (double)acc.x, old.y + (double)acc.y);
+            } else {
+                *o = make_double2((double)acc.x, (double)acc.y);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// res = g - J^T lam with the FP64 Jacobian blocks, by block column
+template <int SW>
+__global__ void __launch_bounds__(256) k_residual_t(PlanDev P, BatchDev B) {
+    const int g = blockIdx.y;
+    if (!B.gsolve[g]) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = tid / SW, lane = tid % SW;
+    if (c >= P.nb) return;
+    const size_t base = (size_t)g * P.nb * SW;
+    const double2 b = B.rhs[base + (size_t)c * SW + lane];
+    Vec2<double> acc = {b.x, b.y};
+    const Blk<double>* A = reinterpret_cast<const Blk<double>*>(B.A64) + (size_t)g * P.n_a * SW;
+    for (int e = P.acol_ptr[c]; e < P.acol_ptr[c + 1]; ++e) {
+        const int2 ar = P.acol[e];
+        const double2 x = B.dx[base + (size_t)ar.y * SW + lane];
+        msubtv(acc, ldb(A + (size_t)ar.x * SW + lane), Vec2<double>{x.x, x.y});
+    }
+    B.res[base + (size_t)c * SW + lane] = make_double2(acc.x, acc.y);
+}
+
+// dL/dP_spec = lambda_P, dL/dQ_spec = lambda_Q (PQ buses), per bus, scenario-major
+template <int SW>
+__global__ void k_adj_out(PlanDev P, BatchDev B, double* dp, double* dq) {
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long)B.n_scen * P.n_bus) return;
+    const int s = (int)(tid / P.n_bus), i = (int)(tid % P.n_bus);
+    const int g = s / SW, lane = s % SW;
+    const int node = P.node_of_bus[i];
+    double a = 0.0, b = 0.0;
+    if (node >= 0) {
+        const double2 l = B.dx[((size_t)g * P.nb + node) * SW + lane];
+        a = l.x;
+        b = P.bus_type[i] == BUS_PQ ? l.y : 0.0;
+    }
+    if (dp) dp[tid] = a;
+    if (dq) dq[tid] = b;
+}
+
+// dL/dr, dL/dx per branch (per unit): -lambda^T dF/dp through the branch's pi stamps with
+// y = 1/(r + jx), dy/dr = -y^2, dy/dx = -j y^2; brp = (r, x, g, b, k, theta) per unit
+template <int SW>
+__global__ void k_adj_branch(PlanDev P, BatchDev B, int m, const int* __restrict__ from,
+                             const int* __restrict__ to, const double* __restrict__ brp,
+                             double* dr, double* dxo) {
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long)B.n_scen * m) return;
+    const int s = (int)(tid / m), b = (int)(tid % m);
+    const int g = s / SW, lane = s % SW;
+    const int f = from[b], t = to[b];
+    double gr = 0.0, gx = 0.0;
+    const double* q = brp + (size_t)b * 6;
+    const double r = q[0], x = q[1], k = q[4], th = q[5];
+    const double z2 = r * r + x * x;
+    if (f >= 0 && t >= 0 && z2 > 0.0) {
+        const double yr = r / z2, yi = -x / z2;
+        const double y2r = yr * yr - yi * yi, y2i = 2.0 * yr * yi;  // y^2
+        double sn, cs;
+        sincos(th, &sn, &cs);
+        const double tr = k * cs, ti = k * sn, k2 = k * k;
+        const double2 vf = B.V[((size_t)g * P.n_bus + f) * SW + lane];
+        const double2 vt = B.V[((size_t)g * P.n_bus + t) * SW + lane];
+        const int nf = P.node_of_bus[f], nt = P.node_of_bus[t];
+        const double2 lf = nf >= 0 ? B.dx[((size_t)g * P.nb + nf) * SW + lane] : make_double2(0, 0);
+        const double2 lt = nt >= 0 ? B.dx[((size_t)g * P.nb + nt) * SW + lane] : make_double2(0, 0);
+        const double lqf = P.bus_type[f] == BUS_PQ ? lf.y : 0.0;
+        const double lqt = P.bus_type[t] == BUS_PQ ? lt.y : 0.0;
+        for (int which = 0; which < 2; ++which) {
+            // dy: -y^2 (r) or -j y^2 (x)
+            const double dyr = which == 0 ? -y2r : y2i, dyi = which == 0 ? -y2i : -y2r;
+            // dYff = dy/k^2, dYtt = dy, dYft = -dy*t/k^2, dYtf = -dy*conj(t)/k^2
+            const double ffr = dyr / k2, ffi = dyi / k2;
+            const double ftr = -(dyr * tr - dyi * ti) / k2, fti = -(dyr * ti + dyi * tr) / k2;
+            const double tfr = -(dyr * tr + dyi * ti) / k2, tfi = -(dyi * tr - dyr * ti) / k2;
+            // dI_f = dYff vf + dYft vt ; dI_t = dYtf vf + dYtt vt
+            const double ifr = ffr * vf.x - ffi * vf.y + ftr * vt.x - fti * vt.y;
+            const double ifi = ffr * vf.y + ffi * vf.x + ftr * vt.y + fti * vt.x;
+            const double itr = tfr * vf.x - tfi * vf.y + dyr * vt.x - dyi * vt.y;
+            const double iti = tfr * vf.y + tfi * vf.x + dyr * vt.y + dyi * vt.x;
+            // dS = V conj(dI)
+            const double sfr = vf.x * ifr + vf.y * ifi, sfi = vf.y * ifr - vf.x * ifi;
+            const double str = vt.x * itr + vt.y * iti, sti = vt.y * itr - vt.x * iti;
+            const double adj = lf.x * sfr + lqf * sfi + lt.x * str + lqt * sti;
+            if (which == 0)
+                gr = -adj;
+            else
+                gx = -adj;
+        }
+    }
+    dr[tid] = gr;
+    dxo[tid] = gx;
 }
 
 }  // namespace gapk

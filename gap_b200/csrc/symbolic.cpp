@@ -317,6 +317,23 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
         P.n_a = na;
     }
     P.slot_a = slot_a;
+    // the same A blocks by block column (row node), for transposed residuals
+    {
+        std::vector<int> cnt(nb + 1, 0);
+        for (int r = 0; r < nb; ++r)
+            for (int e = P.arow_ptr[r]; e < P.arow_ptr[r + 1]; ++e) cnt[P.arow[2 * e + 1] + 1]++;
+        for (int c = 0; c < nb; ++c) cnt[c + 1] += cnt[c];
+        P.acol_ptr = cnt;
+        P.acol.assign(2 * static_cast<size_t>(P.n_a), 0);
+        std::vector<int> fp(cnt.begin(), cnt.end() - 1);
+        for (int r = 0; r < nb; ++r)
+            for (int e = P.arow_ptr[r]; e < P.arow_ptr[r + 1]; ++e) {
+                int c = P.arow[2 * e + 1];
+                int q = fp[c]++;
+                P.acol[2 * q] = P.arow[2 * e];
+                P.acol[2 * q + 1] = r;
+            }
+    }
     // slots that carry Jacobian values, in A order (the fill kernel writes only these)
     P.a_slots.assign(P.n_a, 0);
     for (int sl = 0; sl < P.n_slots; ++sl)

@@ -201,6 +201,25 @@ typedef struct {
 int gapk_nr_solve(gapk_nr_batch b, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
                   void* stream);
 
+/* ==== Adjoint (gradients through the converged state; no counterpart in the reference) ====
+ * With the batch holding a converged state (after gapk_nr_solve, or gapk_nr_stage_load with
+ * the solution as d_v_init), refactorises the Jacobian at that state and solves
+ * J^T lambda = dL/dx, x = (theta of non-slack buses, |V| of PQ buses), with the same block
+ * factors transposed (plus one FP64 refinement step for FP32 batches).  Inputs are dL/d|V|
+ * and dL/dtheta per bus ([n_scen][n_bus]); entries of fixed quantities (slack angle and
+ * magnitude, PV magnitudes) are ignored.  Outputs dL/dP_spec and dL/dQ_spec per bus
+ * ([n_scen][n_bus], per unit; zero where the injection does not enter the equations).  Use a
+ * plan created with GAPK_JAC_EXACT so that the factors are those of the true Jacobian. */
+int gapk_nr_adjoint(gapk_nr_batch b, const double* d_dl_dvm, const double* d_dl_dva,
+                    double* d_dl_dp, double* d_dl_dq, void* stream);
+/* After gapk_nr_adjoint: dL/dr and dL/dx per branch and scenario ([n_scen][n_branch], per
+ * unit), the implicit part -lambda^T dF/d(r, x) through the pi-model stamps.  d_from/d_to are
+ * bus positions (-1 for branches not in the matrix); d_branch_pu = (r, x, g, b, k, theta) per
+ * branch in per unit, as used to build Y. */
+int gapk_nr_adjoint_branch(gapk_nr_batch b, int n_branch, const int* d_from, const int* d_to,
+                           const double* d_branch_pu, double* d_dl_dr, double* d_dl_dx,
+                           void* stream);
+
 /* ==== General sparse LU (ILUSolver) =====================================================
  * Complex square CSR matrices (values interleaved re, im).  Analysis once per pattern on the
  * host: a row permutation giving a zero-free diagonal (maximum transversal), minimum-degree

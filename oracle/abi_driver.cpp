@@ -146,8 +146,29 @@ int main(int argc, char** argv) {
     std::cout << "mismatch_sizes " << mc.size() << " " << mg.size() << "\nmismatch_max_abs_diff "
               << dm << " " << sm << "\n";
 
-    // LU: Y with a dominant diagonal added, reference CPU LU vs plugin LU
-    SparseMatrix A = *Yc;
+    // LU: Y (duplicate entries summed, since the reference LU treats duplicates inconsistently:
+    // last one wins on its dense path, both kept on its sparse path) with a dominant diagonal
+    // added; reference CPU LU vs plugin LU
+    SparseMatrix A;
+    A.num_rows = A.num_cols = n;
+    A.row_ptr.assign(1, 0);
+    for (int i = 0; i < n; ++i) {
+        for (int p = Yc->row_ptr[i]; p < Yc->row_ptr[i + 1]; ++p) {
+            int c = Yc->col_idx[p];
+            bool merged = false;
+            for (int q = A.row_ptr[i]; q < static_cast<int>(A.col_idx.size()); ++q)
+                if (A.col_idx[q] == c) {
+                    A.values[q] += Yc->values[p];
+                    merged = true;
+                }
+            if (!merged) {
+                A.col_idx.push_back(c);
+                A.values.push_back(Yc->values[p]);
+            }
+        }
+        A.row_ptr.push_back(static_cast<int>(A.col_idx.size()));
+    }
+    A.nnz = static_cast<int>(A.values.size());
     double ymax = 0.0;
     for (auto const& v : A.values) ymax = std::max(ymax, std::abs(v));
     for (int i = 0; i < n; ++i)
