@@ -63,9 +63,10 @@ def test_adjoint_matches_fp64_implicit_function_gradient():
 
 
 def test_adjoint_matches_central_finite_differences():
-    """Central differences: h = 1e-6 per unit for P; 1e-5 per unit for Q and 1e-4 of the value
+    """Central differences: h = 1e-6 per unit for P; 1e-4 per unit for Q and 1e-4 of the value
     for r / x, whose gradients are smaller, so that the difference stays above the loss's
-    rounding floor (the FP64 oracle alone shows FD errors up to ~7e-6 at h = 1e-6 on Q)."""
+    rounding floor: the summed loss is O(10-100) MW, so its ~1e-12 rounding noise over 2h swamps
+    small reactive gradients (the FP64 oracle alone shows FD errors ~7e-6 at h = 1e-6 on Q)."""
     import torch
 
     net, s, model, p, q, r, x = _setup(S=2, seed=8, tol=1e-13)
@@ -87,7 +88,7 @@ def test_adjoint_matches_central_finite_differences():
         for _ in range(8 if j < 2 else 6):
             idx = ((int(rng.integers(0, 2)), int(rng.choice(nonslack if j == 0 else pq)))
                    if j < 2 else (int(rng.integers(0, net.n_branch)),))
-            h = (1e-6, 1e-5)[j] if j < 2 else 1e-4 * abs(float(base[j][idx]))
+            h = (1e-6, 1e-4)[j] if j < 2 else 1e-4 * abs(float(base[j][idx]))
             d = torch.zeros_like(base[j])
             d[idx] = h
             plus = list(base)
