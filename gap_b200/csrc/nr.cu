@@ -642,9 +642,9 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
         const size_t N = 2 * (size_t)h.n_tail;
         const size_t smem_max = 232448 - 1024;  // opt-in shared memory per block, less static
         b->dense_w = 0;
-        for (int w : {16, 8}) {
-            size_t bytes = 2 * (size_t)w * dense_ld((int)N) * esz;
-            if (bytes <= smem_max) {
+        for (int w : {32, 16, 8}) {
+            size_t bytes = dense_lu_elems((int)N, w) * esz;
+            if (bytes <= smem_max && (w < 32 || esz == 4 || N <= 200)) {
                 b->dense_w = w;
                 b->dense_smem = bytes;
                 break;
@@ -1086,8 +1086,8 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
     size_t dense_smem = 0;
     int dense_w = 0;
     if (h.n_tail > 0) {
-        for (int w : {16, 8}) {
-            size_t bytes = 2 * (size_t)w * dense_ld((int)N) * 8;
+        for (int w : {32, 16, 8}) {
+            size_t bytes = dense_lu_elems((int)N, w) * 8;
             if (bytes <= 232448 - 1024) {
                 dense_w = w;
                 dense_smem = bytes;

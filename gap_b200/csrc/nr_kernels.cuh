@@ -430,13 +430,39 @@ __global__ void __launch_bounds__(256) k_schur(PlanDev P, BatchDev B) {
     D[(size_t)(r + 1) * ld + c + 1] = acc.d;
 }
 
+// Asynchronous global -> shared copies (cp.async): the copies of one thread are all in flight
+// together, so a staging loop costs one memory latency instead of one per element.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Right-looking blocked LU without pivoting of one scenario's N x N tail (row-major, row
-// stride dense_ld(N), in place).  Each panel of width w <= W (W = 8 or 16) is held TRANSPOSED
-// in shared memory, PT[c][r] = A[k0+r][k0+c], so a column of the panel is contiguous; U12 sits
-// row-major beside it.  The trailing update gives each thread 4x8 register tiles: per k it
-// reads 4 rows of L21 (one vector load) and 8 columns of U12 (two vector loads) for 32 FMAs.
+// stride dense_ld(N), in place), panel width W <= 32:
+//   1. the panel (rows k0.., columns k0..k0+w) is held TRANSPOSED in shared memory,
+//      PT[c][r] = A[k0+r][k0+c], and factored column by column (one barrier per column).  The
+//      same sweep accumulates the inverse of the unit lower triangle,
+//      L11^-1 = M_{w-1} ... M_0 with M_j = I - l_j e_j^T, held transposed in LT[c][r];
+//   2. the trailing columns are processed in chunks of DCW: the A12 chunk is staged in shared
+//      memory (cp.async), U12 = L11^-1 A12 is a small parallel product (each thread up to 8 rows
+//      of one column), kept in shared memory and written back to A;
+//   3. the trailing update: each thread owns 4x8 register tiles and per k reads 4 rows of L21
+//      and 8 columns of U12 (three vector loads) for 32 FMAs.  The trailing matrix is read and
+//      written once per panel.
 // A pivot below 1e-14 in magnitude (the reference LU's tolerance) marks the scenario
-// singular.  Shared memory: 2 * W * dense_ld(N) elements.
+// singular.  Shared memory: dense_lu_smem(N, W) bytes.
+constexpr int DCW = 64;
+
+__host__ __device__ __forceinline__ size_t dense_lu_elems(int N, int W) {
+    return (size_t)W * dense_ld(N) + (size_t)W * DCW + (size_t)W * W;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) k_dense_lu(BatchDev B, int N, int W) {
     const int q = blockIdx.x;
@@ -445,7 +471,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) k_dense_lu(BatchD
     T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* PT = reinterpret_cast<T*>(smraw);
-    T* U = PT + (size_t)W * ld;
+    T* Uc = PT + (size_t)W * ld;
+    T* LT = Uc + (size_t)W * DCW;
     __shared__ int bad;
     const int tid = threadIdx.x, nt = blockDim.x;
     if (tid == 0) bad = 0;
@@ -455,19 +482,22 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) k_dense_lu(BatchD
         const int m = N - k0;
         for (int e = tid; e < m * w; e += nt) {
             const int r = e / w, c = e % w;
-            PT[c * ld + r] = A[(size_t)(k0 + r) * ld + k0 + c];
+            cp_async<sizeof(T)>(PT + c * ld + r, A + (size_t)(k0 + r) * ld + k0 + c);
         }
+        for (int e = tid; e < W * W; e += nt) LT[e] = (e / W == e % W) ? T(1) : T(0);
+        cp_async_wait_all();
         __syncthreads();
+        // panel: at step j, rows j+1.. are eliminated with column j; row j is final
         for (int j = 0; j < w; ++j) {
             const T piv = PT[j * ld + j];
             if (tid == 0 && !(fabs(piv) >= T(1e-14))) bad = 1;
             const T inv = T(1) / piv;
-            for (int r = j + 1 + tid; r < m; r += nt) PT[j * ld + r] *= inv;
-            __syncthreads();
-            const int cols = w - j - 1, rows = m - j - 1;
-            for (int e = tid; e < rows * cols; e += nt) {
-                const int c = j + 1 + e / rows, r = j + 1 + e % rows;
-                PT[c * ld + r] = fma(-PT[j * ld + r], PT[c * ld + j], PT[c * ld + r]);
+            for (int r = j + 1 + tid; r < m; r += nt) {
+                const T l = PT[j * ld + r] * inv;
+                PT[j * ld + r] = l;
+                for (int c = j + 1; c < w; ++c) PT[c * ld + r] = fma(-l, PT[c * ld + j], PT[c * ld + r]);
+                if (r < w)
+                    for (int c = 0; c <= j; ++c) LT[c * W + r] = fma(-l, LT[c * W + j], LT[c * W + r]);
             }
             __syncthreads();
         }
@@ -477,59 +507,91 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) k_dense_lu(BatchD
         }
         const int n2 = N - k0 - w;
         if (n2 > 0) {
-            // U12 = L11^-1 A12, one column per thread; pad columns of U12 to a multiple of 8
-            const int n2p = (n2 + 7) & ~7;
-            for (int c = tid; c < n2p; c += nt) {
-                for (int r = 0; r < w; ++r) {
-                    T v = T(0);
-                    if (c < n2) {
-                        v = A[(size_t)(k0 + r) * ld + k0 + w + c];
-                        for (int qq = 0; qq < r; ++qq) v = fma(-PT[qq * ld + r], U[qq * ld + c], v);
-                        A[(size_t)(k0 + r) * ld + k0 + w + c] = v;
+            const int tr = (m - w + 3) / 4;
+            const int rpt = (w + 3) / 4;  // rows of U12 per thread (<= 8)
+            for (int c0 = 0; c0 < n2; c0 += DCW) {
+                const int cw = min(DCW, n2 - c0);
+                const int cwp = (cw + 7) & ~7;
+                // stage the A12 chunk (cwp columns; the columns past N are row padding and only
+                // ever feed padding columns)
+                {
+                    constexpr int VE = 16 / sizeof(T);
+                    const int vpr = cwp / VE;
+                    for (int e2 = tid; e2 < w * vpr; e2 += nt) {
+                        const int r = e2 / vpr, c = (e2 % vpr) * VE;
+                        cp_async<16>(Uc + r * DCW + c, A + (size_t)(k0 + r) * ld + k0 + w + c0 + c);
                     }
-                    U[r * ld + c] = v;
+                    cp_async_wait_all();
                 }
-            }
-            __syncthreads();
-            // trailing update, rows [w, m), columns [0, n2) of the trailing block
-            const int tr = (m - w + 3) / 4, tcn = n2p / 8;
-            for (int tix = tid; tix < tr * tcn; tix += nt) {
-                const int i0 = w + (tix / tcn) * 4, c0 = (tix % tcn) * 8;
-                T acc[4][8];
+                __syncthreads();
+                // U12 chunk = L11^-1 A12 chunk; thread (g, c) forms rows g*rpt.. of column c
+                {
+                    const int c = tid % DCW, g = tid / DCW, rb = g * rpt;
+                    const bool act = c < cwp && rb < w;
+                    T acc[8];
 #pragma unroll
-                for (int ii = 0; ii < 4; ++ii) {
-                    if (i0 + ii < m) {
-                        const T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + w + c0;
-                        const V4<T> a = ld4(row), b = ld4(row + 4);
+                    for (int i = 0; i < 8; ++i) acc[i] = T(0);
+                    if (act) {
+                        const int qe = min(rb + rpt, w);
+                        for (int qq = 0; qq < qe; ++qq) {
+                            const T a = Uc[qq * DCW + c];
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) {
-                            acc[ii][cc] = a.v[cc];
-                            acc[ii][cc + 4] = b.v[cc];
+                            for (int i = 0; i < 8; ++i)
+                                if (i < rpt) acc[i] = fma(LT[qq * W + rb + i], a, acc[i]);
                         }
-                    } else {
+                    }
+                    __syncthreads();
+                    if (act) {
 #pragma unroll
-                        for (int cc = 0; cc < 8; ++cc) acc[ii][cc] = T(0);
+                        for (int i = 0; i < 8; ++i)
+                            if (i < rpt && rb + i < w) Uc[(rb + i) * DCW + c] = acc[i];
                     }
                 }
-                for (int r = 0; r < w; ++r) {
-                    const V4<T> l = ld4(PT + r * ld + i0);
-                    const V4<T> u0 = ld4(U + r * ld + c0), u1 = ld4(U + r * ld + c0 + 4);
+                __syncthreads();
+                for (int e2 = tid; e2 < w * cw; e2 += nt) {
+                    const int r = e2 / cw, c = e2 % cw;
+                    A[(size_t)(k0 + r) * ld + k0 + w + c0 + c] = Uc[r * DCW + c];
+                }
+                const int tcn = cwp / 8;
+                for (int tix = tid; tix < tr * tcn; tix += nt) {
+                    const int i0 = w + (tix / tcn) * 4, cc0 = (tix % tcn) * 8;
+                    T acc[4][8];
 #pragma unroll
-                    for (int ii = 0; ii < 4; ++ii)
+                    for (int ii = 0; ii < 4; ++ii) {
+                        if (i0 + ii < m) {
+                            const T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + w + c0 + cc0;
+                            const V4<T> a = ld4(row), b = ld4(row + 4);
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) {
-                            acc[ii][cc] = fma(-l.v[ii], u0.v[cc], acc[ii][cc]);
-                            acc[ii][cc + 4] = fma(-l.v[ii], u1.v[cc], acc[ii][cc + 4]);
+                            for (int c = 0; c < 4; ++c) {
+                                acc[ii][c] = a.v[c];
+                                acc[ii][c + 4] = b.v[c];
+                            }
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) acc[ii][c] = T(0);
                         }
-                }
+                    }
+                    for (int r = 0; r < w; ++r) {
+                        const V4<T> l = ld4(PT + r * ld + i0);
+                        const V4<T> u0 = ld4(Uc + r * DCW + cc0), u1 = ld4(Uc + r * DCW + cc0 + 4);
 #pragma unroll
-                for (int ii = 0; ii < 4; ++ii) {
-                    if (i0 + ii < m) {
-                        T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + w + c0;
-                        st4(row, V4<T>{{acc[ii][0], acc[ii][1], acc[ii][2], acc[ii][3]}});
-                        st4(row + 4, V4<T>{{acc[ii][4], acc[ii][5], acc[ii][6], acc[ii][7]}});
+                        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) {
+                                acc[ii][c] = fma(-l.v[ii], u0.v[c], acc[ii][c]);
+                                acc[ii][c + 4] = fma(-l.v[ii], u1.v[c], acc[ii][c + 4]);
+                            }
+                    }
+#pragma unroll
+                    for (int ii = 0; ii < 4; ++ii) {
+                        if (i0 + ii < m) {
+                            T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + w + c0 + cc0;
+                            st4(row, V4<T>{{acc[ii][0], acc[ii][1], acc[ii][2], acc[ii][3]}});
+                            st4(row + 4, V4<T>{{acc[ii][4], acc[ii][5], acc[ii][6], acc[ii][7]}});
+                        }
                     }
                 }
+                __syncthreads();
             }
         }
         __syncthreads();
