@@ -191,7 +191,7 @@ void launch_factor(gapk_nr_batch b, cudaStream_t st) {
     if (P.n_tail > 0) {
         dim3 gs(blocks_for((long)P.n_schur * SW, 256), b->G);
         k_schur<T, SW><<<gs, 256, 0, st>>>(P, B);
-        k_dense_lu<T><<<b->G * SW, 256, b->dense_smem, st>>>(B, 2 * P.n_tail, b->dense_w);
+        launch_dense_lu<T>(b->dense_w, b->G * SW, b->dense_smem, st, B, 2 * P.n_tail);
     }
 }
 
@@ -327,7 +327,7 @@ struct KernelOp {
                 break;
             case 4:
                 if (P.n_tail > 0)
-                    k_dense_lu<T><<<G * SW, 256, b->dense_smem, st>>>(B, 2 * P.n_tail, b->dense_w);
+                    launch_dense_lu<T>(b->dense_w, G * SW, b->dense_smem, st, B, 2 * P.n_tail);
                 break;
             case 5: k_solve_fwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs); break;
             case 6:
@@ -657,18 +657,8 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
         }
         A(b->Dt, L * N * dense_ld((int)N) * esz);
         cudaError_t e = b->precision == GAPK_PREC_FP64
-                            ? cudaFuncSetAttribute(k_dense_lu<double>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)b->dense_smem)
-                            : cudaFuncSetAttribute(k_dense_lu<float>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)b->dense_smem);
-        if (e == cudaSuccess)
-            e = b->precision == GAPK_PREC_FP64
-                    ? cudaFuncSetAttribute(k_dense_lu<double>,
-                                           cudaFuncAttributePreferredSharedMemoryCarveout, 100)
-                    : cudaFuncSetAttribute(k_dense_lu<float>,
-                                           cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+                            ? dense_lu_attributes<double>(b->dense_w, b->dense_smem)
+                            : dense_lu_attributes<float>(b->dense_w, b->dense_smem);
         if (e != cudaSuccess) {
             set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
             return GAPK_ECUDA;
@@ -1026,9 +1016,8 @@ int noalloc_scratch_ptr(void** out) {
     if (!g_noalloc_ptr[dev]) {
         void* p = nullptr;
         GAPK_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        GAPK_CUDA_TRY(cudaFuncSetAttribute(k_dense_lu<double>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           232448 - 1024));
+        for (int w : {32, 16, 8})
+            GAPK_CUDA_TRY(dense_lu_attributes<double>(w, 232448 - 1024));
         g_noalloc_ptr[dev] = p;
     }
     *out = g_noalloc_ptr[dev];
@@ -1190,7 +1179,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
         k_factor<double, 1><<<1, thr, 0, st>>>(P, D);
         if (h.n_tail > 0) {
             k_schur<double, 1><<<blocks_for((long)P.n_schur, 256), 256, 0, st>>>(P, D);
-            k_dense_lu<double><<<1, 256, dense_smem, st>>>(D, (int)N, dense_w);
+            launch_dense_lu<double>(dense_w, 1, dense_smem, st, D, (int)N);
         }
         k_solve_fwd<double, 1><<<1, thr, 0, st>>>(P, D, D.rhs);
         if (h.n_tail > 0)

@@ -444,159 +444,272 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Right-looking blocked LU without pivoting of one scenario's N x N tail (row-major, row
-// stride dense_ld(N), in place), panel width W <= 32:
-//   1. the panel (rows k0.., columns k0..k0+w) is held TRANSPOSED in shared memory,
-//      PT[c][r] = A[k0+r][k0+c], and factored column by column (one barrier per column).  The
-//      same sweep accumulates the inverse of the unit lower triangle,
-//      L11^-1 = M_{w-1} ... M_0 with M_j = I - l_j e_j^T, held transposed in LT[c][r];
-//   2. the trailing columns are processed in chunks of DCW: the A12 chunk is staged in shared
-//      memory (cp.async), U12 = L11^-1 A12 is a small parallel product (each thread up to 8 rows
-//      of one column), kept in shared memory and written back to A;
-//   3. the trailing update: each thread owns 4x8 register tiles and per k reads 4 rows of L21
-//      and 8 columns of U12 (three vector loads) for 32 FMAs.  The trailing matrix is read and
-//      written once per panel.
-// A pivot below 1e-14 in magnitude (the reference LU's tolerance) marks the scenario
-// singular.  Shared memory: dense_lu_smem(N, W) bytes.
-constexpr int DCW = 64;
+// stride dense_ld(N), in place), panels of W columns (W = 8, 16 or 32; compile time):
+//   A. warp 0 factors the W x W diagonal block in registers (lane r holds row r; the pivot
+//      row is broadcast with shuffles) and publishes U11 (transposed, in the panel buffer),
+//      L11 (row-major) and 1/diag(U11) in shared memory;
+//   B. every thread then solves whole rows of L21 (x U11 = a) and whole columns of U12
+//      (L11 y = a), register resident and independent of each other -- two barriers per panel
+//      in all; the L21 rows also go to the transposed panel buffer PT[c][r] for the trailing
+//      update;
+//   C. the trailing update streams U12 through a double-buffered shared-memory chunk of DCW
+//      columns (cp.async prefetch of chunk i+1 during chunk i, one barrier per chunk); each
+//      thread owns 8x8 register tiles and per k reads 8 rows of L21 and 8 columns of U12 (four
+//      vector loads) for 64 FMAs.  The trailing matrix is read and written once per panel.
+// Rows and columns past the last partial panel are padded with the identity, which leaves the
+// factors unchanged.  A pivot below 1e-14 in magnitude (the reference LU's tolerance) marks the
+// scenario singular.  Shared memory: dense_lu_elems(N, W) elements.  The register-resident
+// steps A and B are separate (non-inlined) functions: each then gets the full register budget
+// for its unrolled W-element row, instead of sharing it with the trailing-update tiles.
+constexpr int DCW = 128;
 
 __host__ __device__ __forceinline__ size_t dense_lu_elems(int N, int W) {
-    return (size_t)W * dense_ld(N) + (size_t)W * DCW + (size_t)W * W;
+    return (size_t)W * dense_ld(N) + 2 * (size_t)W * DCW + (size_t)W * (W + 4) + (size_t)W;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) k_dense_lu(BatchDev B, int N, int W) {
+// A: factor the diagonal block A[k0.., k0..] (w <= W rows and columns) in the lanes of one warp.
+// Returns 1 if a pivot is below the tolerance.
+template <typename T, int W>
+__device__ __noinline__ int dense_diag_block(T* A, int ld, int k0, int w, T* PT, T* SL, T* SD) {
+    const int r = threadIdx.x & 31;
+    T a[W];
+    if (r < w) {
+        const T* row = A + (size_t)(k0 + r) * ld + k0;
+#pragma unroll
+        for (int c4 = 0; c4 < W; c4 += 4) {
+            // columns up to ld - 1 lie inside the padded row
+            const V4<T> v = k0 + c4 < ld ? ld4(row + c4) : V4<T>{{T(0), T(0), T(0), T(0)}};
+#pragma unroll
+            for (int t = 0; t < 4; ++t) a[c4 + t] = c4 + t < w ? v.v[t] : T(0);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < W; ++c) a[c] = c == r ? T(1) : T(0);
+    }
+    int badl = 0;
+#pragma unroll
+    for (int kk = 0; kk < W; ++kk) {
+        const T piv = __shfl_sync(0xffffffffu, a[kk], kk);
+        if (kk < w && !(fabs(piv) >= T(1e-14))) badl = 1;
+        const T inv = T(1) / piv;
+        if (r == 0) SD[kk] = inv;
+        const bool below = r > kk;
+        const T l = a[kk] * inv;
+        if (below) a[kk] = l;
+#pragma unroll
+        for (int c = kk + 1; c < W; ++c) {
+            const T u = __shfl_sync(0xffffffffu, a[c], kk);
+            if (below) a[c] = fma(-l, u, a[c]);
+        }
+    }
+    if (r < W) {
+#pragma unroll
+        for (int c = 0; c < W; ++c) PT[c * ld + r] = a[c];  // U11 read as PT[c][k], k <= c
+    }
+    if (r < w) {
+        T* row = A + (size_t)(k0 + r) * ld + k0;
+        if (w == W) {
+#pragma unroll
+            for (int c4 = 0; c4 < W; c4 += 4) st4(row + c4, V4<T>{{a[c4], a[c4 + 1], a[c4 + 2], a[c4 + 3]}});
+        } else {
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+                if (c < w) row[c] = a[c];
+        }
+    }
+    if (r < W) {
+#pragma unroll
+        for (int c = 0; c < W; ++c) SL[r * (W + 4) + c] = a[c];  // L11 row-major, stride W + 4
+    }
+    return badl;
+}
+
+// B, one row of L21: x U11 = a for the row at `row` (W values), written back and to PT[c][r].
+template <typename T, int W>
+__device__ __noinline__ void dense_l21_row(T* row, const T* PT, const T* SD, T* PTr, int ld) {
+    T x[W];
+#pragma unroll
+    for (int c4 = 0; c4 < W; c4 += 4) {
+        const V4<T> v = ld4(row + c4);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) x[c4 + t] = v.v[t];
+    }
+#pragma unroll
+    for (int c = 0; c < W; ++c) {
+        T s0 = x[c], s1 = T(0);
+#pragma unroll
+        for (int k4 = 0; k4 < c; k4 += 4) {
+            const V4<T> u = ld4(PT + c * ld + k4);
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                if (k4 + t < c) {
+                    if (t & 1) s1 = fma(-x[k4 + t], u.v[t], s1);
+                    else s0 = fma(-x[k4 + t], u.v[t], s0);
+                }
+        }
+        x[c] = (s0 + s1) * SD[c];
+    }
+#pragma unroll
+    for (int c = 0; c < W; ++c) PTr[c * ld] = x[c];
+#pragma unroll
+    for (int c4 = 0; c4 < W; c4 += 4) st4(row + c4, V4<T>{{x[c4], x[c4 + 1], x[c4 + 2], x[c4 + 3]}});
+}
+
+// B, one column of U12: L11 y = a (unit lower) for the column at `col` (W values, stride ld),
+// in place; L11 row-major in SL with row stride W + 4.
+template <typename T, int W>
+__device__ __noinline__ void dense_u12_col(T* col, const T* SL, int ld) {
+    T y[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) y[i] = col[(size_t)i * ld];
+#pragma unroll
+    for (int i = 1; i < W; ++i) {
+        T s0 = y[i], s1 = T(0);
+#pragma unroll
+        for (int k4 = 0; k4 < i; k4 += 4) {
+            const V4<T> l = ld4(SL + i * (W + 4) + k4);
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                if (k4 + t < i) {
+                    if (t & 1) s1 = fma(-l.v[t], y[k4 + t], s1);
+                    else s0 = fma(-l.v[t], y[k4 + t], s0);
+                }
+        }
+        y[i] = s0 + s1;
+    }
+#pragma unroll
+    for (int i = 0; i < W; ++i) col[(size_t)i * ld] = y[i];
+}
+
+template <typename T, int W>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchDev B, int N) {
+    static_assert(W == 8 || W == 16 || W == 32, "panel width");
     const int q = blockIdx.x;
     if (q >= B.n_scen || !B.solving[q]) return;
     const int ld = dense_ld(N);
     T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* PT = reinterpret_cast<T*>(smraw);
-    T* Uc = PT + (size_t)W * ld;
-    T* LT = Uc + (size_t)W * DCW;
+    T* PT = reinterpret_cast<T*>(smraw);        // [W][ld]: PT[c*ld + r] = panel (r, c)
+    T* Ub0 = PT + (size_t)W * ld;               // [W][DCW] U12 chunk, two buffers
+    T* Ub1 = Ub0 + W * DCW;
+    T* SL = Ub1 + W * DCW;                      // [W][W + 4] L11 row-major
+    T* SD = SL + W * (W + 4);                         // [W] 1 / U11 diagonal
     __shared__ int bad;
     const int tid = threadIdx.x, nt = blockDim.x;
+    constexpr int VE = 16 / sizeof(T);
     if (tid == 0) bad = 0;
-    __syncthreads();
     for (int k0 = 0; k0 < N; k0 += W) {
         const int w = min(W, N - k0);
         const int m = N - k0;
-        for (int e = tid; e < m * w; e += nt) {
-            const int r = e / w, c = e % w;
-            cp_async<sizeof(T)>(PT + c * ld + r, A + (size_t)(k0 + r) * ld + k0 + c);
+        const int n2 = m - w;  // > 0 only for full panels
+        // ---- A: diagonal block, warp 0
+        if (tid < 32) {
+            if (dense_diag_block<T, W>(A, ld, k0, w, PT, SL, SD)) bad = 1;
         }
-        for (int e = tid; e < W * W; e += nt) LT[e] = (e / W == e % W) ? T(1) : T(0);
-        cp_async_wait_all();
         __syncthreads();
-        // panel: at step j, rows j+1.. are eliminated with column j; row j is final
-        for (int j = 0; j < w; ++j) {
-            const T piv = PT[j * ld + j];
-            if (tid == 0 && !(fabs(piv) >= T(1e-14))) bad = 1;
-            const T inv = T(1) / piv;
-            for (int r = j + 1 + tid; r < m; r += nt) {
-                const T l = PT[j * ld + r] * inv;
-                PT[j * ld + r] = l;
-                for (int c = j + 1; c < w; ++c) PT[c * ld + r] = fma(-l, PT[c * ld + j], PT[c * ld + r]);
-                if (r < w)
-                    for (int c = 0; c <= j; ++c) LT[c * W + r] = fma(-l, LT[c * W + j], LT[c * W + r]);
+        if (n2 > 0) {
+            // ---- B: rows of L21 and columns of U12, one per thread at a time
+            for (int it = tid; it < 2 * n2; it += nt) {
+                if (it < n2) {
+                    const int r = W + it;
+                    dense_l21_row<T, W>(A + (size_t)(k0 + r) * ld + k0, PT, SD, PT + r, ld);
+                } else {
+                    dense_u12_col<T, W>(A + (size_t)k0 * ld + k0 + W + (it - n2), SL, ld);
+                }
             }
             __syncthreads();
-        }
-        for (int e = tid; e < m * w; e += nt) {
-            const int r = e / w, c = e % w;
-            A[(size_t)(k0 + r) * ld + k0 + c] = PT[c * ld + r];
-        }
-        const int n2 = N - k0 - w;
-        if (n2 > 0) {
-            const int tr = (m - w + 3) / 4;
-            const int rpt = (w + 3) / 4;  // rows of U12 per thread (<= 8)
-            for (int c0 = 0; c0 < n2; c0 += DCW) {
-                const int cw = min(DCW, n2 - c0);
-                const int cwp = (cw + 7) & ~7;
-                // stage the A12 chunk (cwp columns; the columns past N are row padding and only
-                // ever feed padding columns)
-                {
-                    constexpr int VE = 16 / sizeof(T);
-                    const int vpr = cwp / VE;
-                    for (int e2 = tid; e2 < w * vpr; e2 += nt) {
-                        const int r = e2 / vpr, c = (e2 % vpr) * VE;
-                        cp_async<16>(Uc + r * DCW + c, A + (size_t)(k0 + r) * ld + k0 + w + c0 + c);
-                    }
-                    cp_async_wait_all();
+            // ---- C: trailing update, U12 in double-buffered chunks
+            const int nch = (n2 + DCW - 1) / DCW;
+            auto stage = [&](int ch, T* buf) {
+                const int c0 = ch * DCW;
+                const int cwp = (min(DCW, n2 - c0) + 7) & ~7;
+                const int vpr = cwp / VE;
+                // the columns past N are row padding and only ever feed padding columns
+                for (int e2 = tid; e2 < W * vpr; e2 += nt) {
+                    const int r = e2 / vpr, c = (e2 % vpr) * VE;
+                    cp_async<16>(buf + r * DCW + c, A + (size_t)(k0 + r) * ld + k0 + W + c0 + c);
                 }
-                __syncthreads();
-                // U12 chunk = L11^-1 A12 chunk; thread (g, c) forms rows g*rpt.. of column c
-                {
-                    const int c = tid % DCW, g = tid / DCW, rb = g * rpt;
-                    const bool act = c < cwp && rb < w;
-                    T acc[8];
+            };
+            stage(0, Ub0);
+            cp_async_wait_all();
+            __syncthreads();
+            const int tr = (n2 + 3) / 4;
+            for (int ch = 0; ch < nch; ++ch) {
+                T* cur = (ch & 1) ? Ub1 : Ub0;
+                if (ch + 1 < nch) stage(ch + 1, (ch & 1) ? Ub0 : Ub1);
+                const int c0 = ch * DCW;
+                const int tcn = ((min(DCW, n2 - c0) + 7) & ~7) / 8;
+                const int tr8 = (n2 + 7) / 8;
+                const int ntile = tr8 * tcn;
+                for (int tix = tid; tix < ntile; tix += nt) {
+                    const int i0 = W + (tix / tcn) * 8, cc0 = (tix % tcn) * 8;
+                    T acc[8][8];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) acc[i] = T(0);
-                    if (act) {
-                        const int qe = min(rb + rpt, w);
-                        for (int qq = 0; qq < qe; ++qq) {
-                            const T a = Uc[qq * DCW + c];
-#pragma unroll
-                            for (int i = 0; i < 8; ++i)
-                                if (i < rpt) acc[i] = fma(LT[qq * W + rb + i], a, acc[i]);
-                        }
-                    }
-                    __syncthreads();
-                    if (act) {
-#pragma unroll
-                        for (int i = 0; i < 8; ++i)
-                            if (i < rpt && rb + i < w) Uc[(rb + i) * DCW + c] = acc[i];
-                    }
-                }
-                __syncthreads();
-                for (int e2 = tid; e2 < w * cw; e2 += nt) {
-                    const int r = e2 / cw, c = e2 % cw;
-                    A[(size_t)(k0 + r) * ld + k0 + w + c0 + c] = Uc[r * DCW + c];
-                }
-                const int tcn = cwp / 8;
-                for (int tix = tid; tix < tr * tcn; tix += nt) {
-                    const int i0 = w + (tix / tcn) * 4, cc0 = (tix % tcn) * 8;
-                    T acc[4][8];
-#pragma unroll
-                    for (int ii = 0; ii < 4; ++ii) {
+                    for (int ii = 0; ii < 8; ++ii) {
                         if (i0 + ii < m) {
-                            const T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + w + c0 + cc0;
+                            const T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + W + c0 + cc0;
                             const V4<T> a = ld4(row), b = ld4(row + 4);
 #pragma unroll
-                            for (int c = 0; c < 4; ++c) {
-                                acc[ii][c] = a.v[c];
-                                acc[ii][c + 4] = b.v[c];
-                            }
+                            for (int c = 0; c < 4; ++c) { acc[ii][c] = a.v[c]; acc[ii][c + 4] = b.v[c]; }
                         } else {
 #pragma unroll
                             for (int c = 0; c < 8; ++c) acc[ii][c] = T(0);
                         }
                     }
-                    for (int r = 0; r < w; ++r) {
-                        const V4<T> l = ld4(PT + r * ld + i0);
-                        const V4<T> u0 = ld4(Uc + r * DCW + cc0), u1 = ld4(Uc + r * DCW + cc0 + 4);
+#pragma unroll 2
+                    for (int r = 0; r < W; ++r) {
+                        const V4<T> l0 = ld4(PT + r * ld + i0), l1 = ld4(PT + r * ld + i0 + 4);
+                        const V4<T> u0 = ld4(cur + r * DCW + cc0), u1 = ld4(cur + r * DCW + cc0 + 4);
 #pragma unroll
                         for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
                             for (int c = 0; c < 4; ++c) {
-                                acc[ii][c] = fma(-l.v[ii], u0.v[c], acc[ii][c]);
-                                acc[ii][c + 4] = fma(-l.v[ii], u1.v[c], acc[ii][c + 4]);
+                                acc[ii][c] = fma(-l0.v[ii], u0.v[c], acc[ii][c]);
+                                acc[ii][c + 4] = fma(-l0.v[ii], u1.v[c], acc[ii][c + 4]);
+                                acc[ii + 4][c] = fma(-l1.v[ii], u0.v[c], acc[ii + 4][c]);
+                                acc[ii + 4][c + 4] = fma(-l1.v[ii], u1.v[c], acc[ii + 4][c + 4]);
                             }
                     }
 #pragma unroll
-                    for (int ii = 0; ii < 4; ++ii) {
+                    for (int ii = 0; ii < 8; ++ii) {
                         if (i0 + ii < m) {
-                            T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + w + c0 + cc0;
+                            T* row = A + (size_t)(k0 + i0 + ii) * ld + k0 + W + c0 + cc0;
                             st4(row, V4<T>{{acc[ii][0], acc[ii][1], acc[ii][2], acc[ii][3]}});
                             st4(row + 4, V4<T>{{acc[ii][4], acc[ii][5], acc[ii][6], acc[ii][7]}});
                         }
                     }
                 }
+                cp_async_wait_all();
                 __syncthreads();
             }
         }
-        __syncthreads();
     }
     if (tid == 0 && bad) B.singular[q] = 1;
+}
+
+// Host side: opt in to the kernel's shared memory and launch it for panel width W.
+template <typename T>
+cudaError_t dense_lu_attributes(int W, size_t smem) {
+    auto set = [&](auto fn) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        return e;
+    };
+    switch (W) {
+        case 32: return set(k_dense_lu<T, 32>);
+        case 16: return set(k_dense_lu<T, 16>);
+        case 8: return set(k_dense_lu<T, 8>);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <typename T>
+void launch_dense_lu(int W, int grid, size_t smem, cudaStream_t st, BatchDev const& B, int N) {
+    switch (W) {
+        case 32: k_dense_lu<T, 32><<<grid, 256, smem, st>>>(B, N); break;
+        case 16: k_dense_lu<T, 16><<<grid, 256, smem, st>>>(B, N); break;
+        case 8: k_dense_lu<T, 8><<<grid, 256, smem, st>>>(B, N); break;
+    }
 }
 
 // Forward (unit L) then backward (U) substitution on one scenario's tail vector, blocked by
