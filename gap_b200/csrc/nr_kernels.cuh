@@ -144,6 +144,7 @@ __global__ void __launch_bounds__(256) k_mismatch(PlanDev P, BatchDev B) {
         const int pb = P.y_row_ptr[i], pe = P.y_row_ptr[i + 1];
         double ir = 0.0, ii = 0.0;
         if (B.y_shared) {
+#pragma unroll 4
             for (int p = pb; p < pe; ++p) {
                 const double2 y = B.Y[p];
                 const double2 v = Vg[(size_t)P.y_col[p] * SW + lane];
@@ -154,6 +155,7 @@ __global__ void __launch_bounds__(256) k_mismatch(PlanDev P, BatchDev B) {
             }
         } else {
             const double2* Yg = B.Y + (size_t)g * P.nnz_y * SW;
+#pragma unroll 4
             for (int p = pb; p < pe; ++p) {
                 const double2 y = Yg[(size_t)p * SW + lane];
                 const double2 v = Vg[(size_t)P.y_col[p] * SW + lane];
@@ -276,6 +278,7 @@ __global__ void __launch_bounds__(256) k_jfill(PlanDev P, BatchDev B) {
     const bool diag = si.x == si.y;
     if (diag || si.z < si.w) {
         double G = 0.0, Bv = 0.0;
+#pragma unroll 4
         for (int e = si.z; e < si.w; ++e) {
             const int p = P.slot_src[e];
             const double2 y = B.y_shared ? B.Y[p] : B.Y[((size_t)g * P.nnz_y + p) * SW + lane];
@@ -352,6 +355,7 @@ __global__ void k_factor(PlanDev P, BatchDev B) {
         for (int t = ta + e0; t < tb; t += ne) {
             const int4 tg = P.targets[t];
             Blk<T> acc = (tg.w & 2) ? ldb(F + (size_t)tg.x * SW + lane) : Blk<T>{0, 0, 0, 0};
+#pragma unroll 4
             for (int p = tg.y; p < tg.z; ++p) {
                 const int2 pr = P.pairs[p];
                 msub(acc, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
@@ -416,6 +420,7 @@ __global__ void __launch_bounds__(256) k_schur(PlanDev P, BatchDev B) {
     const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
     const int4 tg = P.schur[t];
     Blk<T> acc = (tg.w >> 30) ? ldb(F + (size_t)tg.x * SW + lane) : Blk<T>{0, 0, 0, 0};
+#pragma unroll 4
     for (int p = tg.y; p < tg.z; ++p) {
         const int2 pr = P.pairs[p];
         msub(acc, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
@@ -814,6 +819,7 @@ __global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ r
             const int k = P.level_nodes[t];
             const double2 b = R[(size_t)k * SW + lane];
             Vec2<T> acc = {(T)b.x, (T)b.y};
+#pragma unroll 4
             for (int q = P.rptr[k]; q < P.rptr[k + 1]; ++q) {
                 const int2 r = P.rlist[q];
                 msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
@@ -825,6 +831,7 @@ __global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ r
     for (int k = P.ns + e0; k < P.nb; k += ne) {
         const double2 b = R[(size_t)k * SW + lane];
         Vec2<T> acc = {(T)b.x, (T)b.y};
+#pragma unroll 4
         for (int q = P.rptr[k]; q < P.rptr[k + 1]; ++q) {
             const int2 r = P.rlist[q];
             msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
@@ -847,6 +854,7 @@ __global__ void k_solve_bwd(PlanDev P, BatchDev B, double2* out, int accumulate)
         for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
             const int k = P.level_nodes[t];
             Vec2<T> acc = ldv(X + (size_t)k * SW + lane);
+#pragma unroll 4
             for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
                 msubv(acc, ldb(F + (size_t)(Ub + p) * SW + lane),
                       ldv(X + (size_t)P.lidx[p] * SW + lane));
@@ -877,6 +885,7 @@ __global__ void __launch_bounds__(256) k_residual(PlanDev P, BatchDev B) {
     const double2 b = B.rhs[base + (size_t)k * SW + lane];
     Vec2<double> acc = {b.x, b.y};
     const Blk<double>* A = reinterpret_cast<const Blk<double>*>(B.A64) + (size_t)g * P.n_a * SW;
+#pragma unroll 4
     for (int e = P.arow_ptr[k]; e < P.arow_ptr[k + 1]; ++e) {
         const int2 ac = P.arow[e];
         const double2 x = B.dx[base + (size_t)ac.y * SW + lane];
@@ -1031,6 +1040,7 @@ __global__ void k_solve_fwd_t(PlanDev P, BatchDev B, const double2* __restrict__
             const int j = P.level_nodes[t];
             const double2 b = R[(size_t)j * SW + lane];
             Vec2<T> acc = {(T)b.x, (T)b.y};
+#pragma unroll 4
             for (int q = P.rptr[j]; q < P.rptr[j + 1]; ++q) {
                 const int2 r = P.rlist[q];  // (L slot of (j,k), k); U(k,j) sits nnz_l further
                 msubtv(acc, ldb(F + (size_t)(r.x + P.nnz_l) * SW + lane),
@@ -1043,6 +1053,7 @@ __global__ void k_solve_fwd_t(PlanDev P, BatchDev B, const double2* __restrict__
     for (int j = P.ns + e0; j < P.nb; j += ne) {
         const double2 b = R[(size_t)j * SW + lane];
         Vec2<T> acc = {(T)b.x, (T)b.y};
+#pragma unroll 4
         for (int q = P.rptr[j]; q < P.rptr[j + 1]; ++q) {
             const int2 r = P.rlist[q];
             msubtv(acc, ldb(F + (size_t)(r.x + P.nnz_l) * SW + lane),
@@ -1148,6 +1159,7 @@ __global__ void k_solve_bwd_t(PlanDev P, BatchDev B, double2* out, int accumulat
         for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
             const int k = P.level_nodes[t];
             Vec2<T> acc = ldv(X + (size_t)k * SW + lane);
+#pragma unroll 4
             for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
                 msubtv(acc, ldb(F + (size_t)(P.nb + p) * SW + lane),
                        ldv(X + (size_t)P.lidx[p] * SW + lane));
@@ -1177,6 +1189,7 @@ __global__ void __launch_bounds__(256) k_residual_t(PlanDev P, BatchDev B) {
     const double2 b = B.rhs[base + (size_t)c * SW + lane];
     Vec2<double> acc = {b.x, b.y};
     const Blk<double>* A = reinterpret_cast<const Blk<double>*>(B.A64) + (size_t)g * P.n_a * SW;
+#pragma unroll 4
     for (int e = P.acol_ptr[c]; e < P.acol_ptr[c + 1]; ++e) {
         const int2 ar = P.acol[e];
         const double2 x = B.dx[base + (size_t)ar.y * SW + lane];
