@@ -805,26 +805,83 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
 // node gathers its sparse contributions; U x = y over the sparse levels (descending) once
 // the dense tail is solved.  x is written as FP64 (optionally added to `out`).
 // ---------------------------------------------------------------------------------------
+// Levels with few nodes split every row over s sub-slots (s a power of two, up to 32): the
+// sub-slots of one warp reduce with shuffles, the warps of one row through shared memory.
+// split_factor: the largest s <= 32 with c * s <= ne (at least 1).
+__device__ __forceinline__ int split_factor(int c, int ne) {
+    int s = 1;
+    while (s < 32 && c * s * 2 <= ne) s *= 2;
+    return s;
+}
+
+// Sum `acc` over the s sub-slots of each row (slot e0 = row * s + sub); the result is valid in
+// sub-slot 0.  Every thread of the block calls this (uniform s).
+template <typename T, int SW>
+__device__ __forceinline__ Vec2<T> split_reduce(Vec2<T> acc, int s, int sub, int row, int lane,
+                                                Vec2<T>* red) {
+    constexpr int S = 32 / SW;  // slots per warp
+    const int sw = s < S ? s : S;
+    for (int d = 1; d < sw; d *= 2) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, d * SW);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, d * SW);
+    }
+    if (s > S) {
+        const int parts = s / S;
+        if (sub % S == 0) red[(row * parts + sub / S) * SW + lane] = acc;
+        __syncthreads();
+        if (sub == 0) {
+            acc = red[(row * parts) * SW + lane];
+            for (int w = 1; w < parts; ++w) {
+                const Vec2<T> v = red[(row * parts + w) * SW + lane];
+                acc.x += v.x;
+                acc.y += v.y;
+            }
+        }
+    }
+    return acc;
+}
+
 template <typename T, int SW>
 __global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ rhs) {
     const int g = blockIdx.x;
     if (!B.gsolve[g]) return;
+    __shared__ Vec2<T> red[256];  // (blockDim / (32 / SW)) partial sums, <= 256 for SW <= 8
     const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
     Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
     const double2* R = rhs + (size_t)g * P.nb * SW;
     const int lane = threadIdx.x % SW;
     const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
     for (int h = 0; h < P.n_levels; ++h) {
-        for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
-            const int k = P.level_nodes[t];
-            const double2 b = R[(size_t)k * SW + lane];
-            Vec2<T> acc = {(T)b.x, (T)b.y};
+        const int lb = P.level_ptr[h], c = P.level_ptr[h + 1] - lb;
+        const int s = split_factor(c, ne);
+        if (s == 1) {
+            for (int t = lb + e0; t < lb + c; t += ne) {
+                const int k = P.level_nodes[t];
+                const double2 b = R[(size_t)k * SW + lane];
+                Vec2<T> acc = {(T)b.x, (T)b.y};
 #pragma unroll 4
-            for (int q = P.rptr[k]; q < P.rptr[k + 1]; ++q) {
-                const int2 r = P.rlist[q];
-                msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
+                for (int q = P.rptr[k]; q < P.rptr[k + 1]; ++q) {
+                    const int2 r = P.rlist[q];
+                    msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
+                }
+                stv(X + (size_t)k * SW + lane, acc);
             }
-            stv(X + (size_t)k * SW + lane, acc);
+        } else {
+            const int j = e0 / s, sub = e0 % s;
+            const int k = j < c ? P.level_nodes[lb + j] : 0;
+            Vec2<T> acc = {T(0), T(0)};
+            if (j < c) {
+#pragma unroll 4
+                for (int q = P.rptr[k] + sub; q < P.rptr[k + 1]; q += s) {
+                    const int2 r = P.rlist[q];
+                    msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
+                }
+            }
+            acc = split_reduce<T, SW>(acc, s, sub, j, lane, red);
+            if (j < c && sub == 0) {
+                const double2 b = R[(size_t)k * SW + lane];
+                stv(X + (size_t)k * SW + lane, Vec2<T>{(T)b.x + acc.x, (T)b.y + acc.y});
+            }
         }
         __syncthreads();
     }
@@ -844,29 +901,53 @@ template <typename T, int SW>
 __global__ void k_solve_bwd(PlanDev P, BatchDev B, double2* out, int accumulate) {
     const int g = blockIdx.x;
     if (!B.gsolve[g]) return;
+    __shared__ Vec2<T> red[256];
     const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
     Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
     double2* O = out + (size_t)g * P.nb * SW;
     const int lane = threadIdx.x % SW;
     const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
     const int Ub = P.nb + P.nnz_l;
+    auto finish = [&](int k, Vec2<T> acc) {
+        const Vec2<T> x = mulv(ldb(F + (size_t)k * SW + lane), acc);
+        stv(X + (size_t)k * SW + lane, x);
+        double2* o = O + (size_t)k * SW + lane;
+        if (accumulate) {
+            const double2 old = *o;
+            *o = make_double2(old.x + (double)x.x, old.y + (double)x.y);
+        } else {
+            *o = make_double2((double)x.x, (double)x.y);
+        }
+    };
     for (int h = P.n_levels - 1; h >= 0; --h) {
-        for (int t = P.level_ptr[h] + e0; t < P.level_ptr[h + 1]; t += ne) {
-            const int k = P.level_nodes[t];
-            Vec2<T> acc = ldv(X + (size_t)k * SW + lane);
+        const int lb = P.level_ptr[h], c = P.level_ptr[h + 1] - lb;
+        const int s = split_factor(c, ne);
+        if (s == 1) {
+            for (int t = lb + e0; t < lb + c; t += ne) {
+                const int k = P.level_nodes[t];
+                Vec2<T> acc = ldv(X + (size_t)k * SW + lane);
 #pragma unroll 4
-            for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
-                msubv(acc, ldb(F + (size_t)(Ub + p) * SW + lane),
-                      ldv(X + (size_t)P.lidx[p] * SW + lane));
+                for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
+                    msubv(acc, ldb(F + (size_t)(Ub + p) * SW + lane),
+                          ldv(X + (size_t)P.lidx[p] * SW + lane));
+                }
+                finish(k, acc);
             }
-            const Vec2<T> x = mulv(ldb(F + (size_t)k * SW + lane), acc);
-            stv(X + (size_t)k * SW + lane, x);
-            double2* o = O + (size_t)k * SW + lane;
-            if (accumulate) {
-                const double2 old = *o;
-                *o = make_double2(old.x + (double)x.x, old.y + (double)x.y);
-            } else {
-                *o = make_double2((double)x.x, (double)x.y);
+        } else {
+            const int j = e0 / s, sub = e0 % s;
+            const int k = j < c ? P.level_nodes[lb + j] : 0;
+            Vec2<T> acc = {T(0), T(0)};
+            if (j < c) {
+#pragma unroll 4
+                for (int p = P.lptr[k] + sub; p < P.lptr[k + 1]; p += s) {
+                    msubv(acc, ldb(F + (size_t)(Ub + p) * SW + lane),
+                          ldv(X + (size_t)P.lidx[p] * SW + lane));
+                }
+            }
+            acc = split_reduce<T, SW>(acc, s, sub, j, lane, red);
+            if (j < c && sub == 0) {
+                const Vec2<T> xk = ldv(X + (size_t)k * SW + lane);
+                finish(k, Vec2<T>{xk.x + acc.x, xk.y + acc.y});
             }
         }
         __syncthreads();
