@@ -419,6 +419,9 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
         });
         for (int s : lvl_slots) {
             auto pe = emit(s);
+            // a slot with its Jacobian value and nothing to subtract or invert is final as
+            // filled: no target
+            if (pe.first == pe.second && s >= nb && slot_a[s] >= 0) continue;
             P.targets.push_back(s);
             P.targets.push_back(pe.first);
             P.targets.push_back(pe.second);
