@@ -8,10 +8,20 @@ whole Newton loop on the device (CUDA graph with a device-side while node).  Wea
 every rank solves its own 1024 scenarios of the same grid.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --workload mixed     # the mixed batch below, one JSON line
+    python bench.py --workload large     # the 100k-bus grid below, one JSON line
 
 Prints one JSON line (rank 0).  `value` times the solve with inputs resident in HBM; `e2e`
 times the same call with host (pinned) inputs and results copied inside the timed region.
 The plain FP64 single-scenario solve of the same grid is reported beside it.
+
+Supplementary workloads (one GPU, not the headline):
+  mixed  1024 load scenarios of a 2k-bus grid of the same generator, 256 N-1 branch outages
+         of that grid (distinct non-bridge branches, one plan shared with the load scenarios),
+         and 64 independent grids with n log-uniform in [500, 20000], all solved concurrently
+         (one CUDA stream and graph per study, lanes/threads autotuned per study).
+  large  32 load scenarios of a 100k-bus grid of the same generator (accuracy against the
+         FP64 oracle: tests/test_gpu_large.py, run with GAP_B200_LARGE=1).
 """
 
 from __future__ import annotations
@@ -446,6 +456,127 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------------------------------
+# supplementary workloads
+# ------------------------------------------------------------------------------------------
+
+def run_mixed(args):
+    import numpy as np
+    import torch
+
+    from gap_b200 import studies, synth
+
+    t0 = time.perf_counter()
+    net = synth.transmission_grid(GRID_SEED, n=2000)
+    v0 = synth.dc_start(net, BASE)
+    s_load = synth.load_scenarios(net, 1024, sigma=SIGMA, seed=1, base_power=BASE)
+    load = studies.load_study("load", net, s_load, v0, base_power=BASE)
+    outs = synth.n_minus_1(net, 256)
+    cont = studies.contingency_study("n-1", net, outs, net.specified_power(BASE), v0,
+                                     base_power=BASE, plan=load.plan)
+    grids = []
+    for i, n in enumerate(synth.grid_sizes(64)):
+        g = synth.transmission_grid(100 + i, n=int(n))
+        grids.append(studies.load_study(f"grid{i}", g, g.specified_power(BASE)[None],
+                                        synth.dc_start(g, BASE), base_power=BASE))
+    setup_s = time.perf_counter() - t0
+    all_st = [load, cont] + grids
+    kw = dict(tol=TOL, max_iter=MAX_ITER, policy="newton", refine=1)
+    t1 = time.perf_counter()
+    for st in all_st:
+        studies.autotune(st, **kw)
+    tune_s = time.perf_counter() - t1
+    with Clocks(0) as clk:
+        ms, conv, wall = studies.timed_concurrent(all_st, steps=args.steps,
+                                                  warmup=max(args.warmup, 1), **kw)
+    n_sys = sum(st.n_scen for st in all_st)
+    not_conv = {st.name: int((st.result.status != 0).sum().item()) for st in all_st
+                if int((st.result.status != 0).sum().item())}
+    picks = {}
+    for st in all_st:
+        key = f"{st.lanes}x{st.threads}"
+        picks[key] = picks.get(key, 0) + 1
+    # each study alone, for the concurrency gain
+    seq = 0.0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for st in all_st:
+        e0.record()
+        st.batch.solve(st.y, st.s_spec, v_init=st.v0, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        seq += e0.elapsed_time(e1)
+    line = {
+        "metric": "Power-flow solves/s on 1 B200, mixed batch (load scenarios + N-1 + "
+                  "independent grids) at 1e-8 pu",
+        "workload": "mixed", "value": conv / (ms / 1e3), "unit": "solves/s", "n_gpus": 1,
+        "steps": args.steps, "ms_per_step": ms, "converged_per_step": conv,
+        "systems_per_step": n_sys, "not_converged": not_conv, "higher_is_better": True,
+        "dtype": "fp32+fp64",
+        "data": "synthetic (seeded generator, no external dataset)",
+        "config": {"workload": "1024 load scenarios + 256 N-1 outages of a 2000-bus grid "
+                               "+ 64 independent grids, n log-uniform in [500, 20000]",
+                   "grid_sizes": [int(g.net.n_bus) for g in grids],
+                   "tol_pu": TOL, "max_iter": MAX_ITER, "policy": "newton",
+                   "precision": "fp32 factor+solve, fp64 mismatch/update, 1 refine",
+                   "streams": len(all_st), "autotuned_lanes_x_threads": picks,
+                   "autotuned_load_and_n-1": [f"{st.lanes}x{st.threads}" for st in all_st[:2]]},
+        "sequential_ms": seq, "concurrency_gain": seq / ms,
+        "host_wall_ms_per_step": wall * 1e3, "setup_seconds": setup_s,
+        "autotune_seconds": tune_s, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_large(args):
+    import numpy as np
+    import torch
+
+    from gap_b200 import studies, synth
+
+    t0 = time.perf_counter()
+    net = synth.transmission_grid(GRID_SEED, n=100_000)
+    v0 = synth.dc_start(net, BASE)
+    S = 32
+    s_load = synth.load_scenarios(net, S, sigma=SIGMA, seed=1, base_power=BASE)
+    gen_s = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    st = studies.load_study("large", net, s_load, v0, base_power=BASE)
+    plan_s = time.perf_counter() - t1
+    st.lanes, st.threads = 8, 1024
+    b = st.make_batch()
+    kw = dict(tol=TOL, max_iter=MAX_ITER, policy="newton", refine=1)
+    r = b.solve(st.y, st.s_spec, v_init=st.v0, **kw)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            r = b.solve(st.y, st.s_spec, v_init=st.v0, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    status = r.status.cpu().numpy()
+    iters = r.iterations.cpu().numpy()
+    info = st.plan.info
+    line = {
+        "metric": "Power-flow solves/s on 1 B200, 100k-bus grid, FP32 factor + FP64 refinement "
+                  "at 1e-8 pu",
+        "workload": "large", "value": int((status == 0).sum()) / (ms / 1e3),
+        "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "ms_per_step": ms,
+        "higher_is_better": True, "dtype": "fp32+fp64",
+        "data": "synthetic (seeded generator, no external dataset)",
+        "config": {"workload": "32 load scenarios x 100000-bus transmission grid (seed 0)",
+                   "n_tail": info["n_tail"], "nnz_l_blocks": info["nnz_l_blocks"],
+                   "n_pairs": info["n_pairs"], "n_schur_pairs": info["n_schur_pairs"]},
+        "converged": int((status == 0).sum()), "iterations_max": int(iters.max()),
+        "device_bytes": b.device_bytes,
+        "generate_seconds": gen_s, "plan_seconds": plan_s, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_SCEN
     ap = argparse.ArgumentParser()
@@ -456,6 +587,9 @@ def main():
     ap.add_argument("--scenarios", type=int, default=N_SCEN,
                     help="scenarios per GPU (profiling runs use fewer; the headline uses 1024)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling)")
+    ap.add_argument("--workload", default="transmission",
+                    choices=["transmission", "mixed", "large"],
+                    help="transmission: the headline; mixed / large: supplementary lines")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Newton loop from the host instead of one CUDA graph with a "
                          "conditional node (same kernels and work; lets ncu see every launch)")
@@ -470,6 +604,9 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
+    if args.workload != "transmission":
+        (run_mixed if args.workload == "mixed" else run_large)(args)
+        return
     if world > 1:
         import datetime
 

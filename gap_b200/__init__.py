@@ -3,7 +3,8 @@
 A drop-in GPU backend for the reference's Newton-Raphson path (Y-bus assembly, fused
 mismatch, Jacobian fill, sparse block LU, voltage update), computed by hand-written sm_100a
 kernels in libgapk.so.  See `gap_b200.api` for the reference-facing functions and
-`gap_b200.batch` for batched / mixed-precision / differentiable solves.
+`gap_b200.engine` for batched / mixed-precision solves, `gap_b200.autograd` for
+differentiable ones and `gap_b200.studies` for mixed batches of grids and contingencies.
 """
 
 from .network import GENERIC, LINE, LOADGEN, PQ, PV, SHUNT, SLACK, SOURCE, TRAFO, Network

@@ -178,3 +178,41 @@ def test_sparse_lu_analysis_matching_and_errors():
         rp = np.zeros(n + 1, np.int32)
         np.add.at(rp, rows + 1, 1)
         assert SparseLU(np.cumsum(rp), cols).n == n
+
+
+def test_contingency_params_equal_branch_outage():
+    """An N-1 outage expressed as zero r1/x1/g1/b1 (the Y-bus builder's zero-admittance
+    branch) gives the Y values of the network with that branch out of service, and the
+    candidates are exactly the non-bridge branches (checked by removing each one)."""
+    import dataclasses
+
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import connected_components
+
+    from gap_b200 import studies, synth
+
+    net = synth.transmission_grid(6, n=120)
+    outs = synth.n_minus_1(net, 10, seed=4)
+    params = studies.contingency_branch_params(net, outs)
+    f, t, valid = net.branch_index()
+    for s, b in enumerate(outs):
+        keep = valid.copy()
+        keep[b] = False
+        g = sp.coo_matrix((np.ones(keep.sum()), (f[keep], t[keep])), shape=(net.n_bus,) * 2)
+        assert connected_components(g, directed=False)[0] == 1
+        zeroed = dataclasses.replace(net, r1=params[s, :, 0], x1=params[s, :, 1],
+                                     g1=params[s, :, 2], b1=params[s, :, 3])
+        rp, ci, va = restate.ybus_pi(zeroed)
+        A = sp.csr_matrix((va, ci, rp), shape=(net.n_bus,) * 2).toarray()
+        rp2, ci2, va2 = restate.ybus_pi(studies.outage_network(net, b))
+        B = sp.csr_matrix((va2, ci2, rp2), shape=(net.n_bus,) * 2).toarray()
+        assert np.array_equal(A, B)
+        others = np.delete(np.arange(net.n_branch), b)
+        assert np.array_equal(params[s, others], studies.branch_params(net)[others])
+    # every non-candidate in-service branch is a bridge
+    br = synth.bridges(net.n_bus, f[valid], t[valid])
+    for e in np.nonzero(valid)[0][br][:5]:
+        keep = valid.copy()
+        keep[e] = False
+        g = sp.coo_matrix((np.ones(keep.sum()), (f[keep], t[keep])), shape=(net.n_bus,) * 2)
+        assert connected_components(g, directed=False)[0] > 1
