@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(LIB_DIR, "libgapk.so")
 
 GAPK_OK = 0
 PREC_FP64, PREC_FP32 = 0, 1
-POLICY_REFERENCE, POLICY_NEWTON = 0, 1
+POLICY_REFERENCE, POLICY_NEWTON, POLICY_CLAMPED = 0, 1, 2
 JAC_REFERENCE, JAC_EXACT = 0, 1
 ORDER_MINDEG, ORDER_NATURAL = 0, 1
 YBUS_REFERENCE, YBUS_TAPS = 0, 1

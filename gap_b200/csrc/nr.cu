@@ -450,7 +450,7 @@ int load_inputs(gapk_nr_batch b, const gapk_nr_inputs* in, cudaStream_t st) {
         return GAPK_EINVAL;
     }
     if (in->max_iterations < 0 || in->refine < 0 || in->refine > 8 ||
-        (in->policy != GAPK_POLICY_REFERENCE && in->policy != GAPK_POLICY_NEWTON)) {
+        (in->policy < GAPK_POLICY_REFERENCE || in->policy > GAPK_POLICY_CLAMPED)) {
         set_error("inputs: bad max_iterations / refine / policy");
         return GAPK_EINVAL;
     }
@@ -1042,7 +1042,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
         return GAPK_EINVAL;
     }
     if (in->max_iterations < 0 || in->refine != 0 ||
-        (in->policy != GAPK_POLICY_REFERENCE && in->policy != GAPK_POLICY_NEWTON)) {
+        (in->policy < GAPK_POLICY_REFERENCE || in->policy > GAPK_POLICY_CLAMPED)) {
         set_error("gapk_nr_solve_noalloc: bad max_iterations / policy, or refine != 0 "
                   "(this entry point solves in FP64 only)");
         return GAPK_EINVAL;

@@ -1007,17 +1007,19 @@ __global__ void __launch_bounds__(256) k_update(PlanDev P, BatchDev B) {
     const size_t o = ((size_t)g * n + i) * SW + lane;
     double2 v = B.V[o];
     const bool pq = P.bus_type[i] == BUS_PQ;
-    if (B.ctrl[3] == 0) {
-        // reference policy (cpu_newton_raphson.cpp:457-503)
+    if (B.ctrl[3] != 1) {
+        // reference policy (cpu_newton_raphson.cpp:457-503): damping 0.9 and the clamps;
+        // clamped policy: the same clamps and order with the full step
+        const double damp = B.ctrl[3] == 0 ? 0.9 : 1.0;
         const double vm = hypot(v.x, v.y);
-        double a = 0.9 * d.x;
+        double a = damp * d.x;
         if (fabs(a) > 0.15) a = 0.15 * (a > 0 ? 1.0 : -1.0);
         double sn, cs;
         sincos(atan2(v.y, v.x) + a, &sn, &cs);
         v = make_double2(vm * cs, vm * sn);
         if (pq) {
             const double vm0 = hypot(v.x, v.y);
-            double c = 0.9 * d.y;
+            double c = damp * d.y;
             if (fabs(c) > 0.08) c = 0.08 * (c > 0 ? 1.0 : -1.0);
             double vmn = vm0 + c;
             vmn = (vmn < 0.5) ? 0.5 : vmn;

@@ -202,7 +202,8 @@ class NRBatch:
         return int(N.lib().gapk_nr_batch_device_bytes(self._h))
 
     def _inputs(self, y, s_spec, v_init, u_pu, tol, max_iter, policy, refine):
-        pol = N.POLICY_REFERENCE if policy == "reference" else N.POLICY_NEWTON
+        pol = {"reference": N.POLICY_REFERENCE, "newton": N.POLICY_NEWTON,
+               "clamped": N.POLICY_CLAMPED}[policy]
         return N.Inputs(_dptr(y), _dptr(s_spec), _dptr(v_init), _dptr(u_pu), float(tol),
                         int(max_iter), pol, int(refine))
 

@@ -178,6 +178,7 @@ int64_t gapk_nr_batch_device_bytes(gapk_nr_batch b);
 #define GAPK_POLICY_REFERENCE 0 /* damping 0.9, |dtheta|<=0.15, |d|V||<=0.08, |V| in [0.5,1.5]
                                    (cpu_newton_raphson.cpp:438-504)                         */
 #define GAPK_POLICY_NEWTON 1    /* full Newton step                                         */
+#define GAPK_POLICY_CLAMPED 2   /* full Newton step with the reference policy's clamps and |V| clip  */
 
 typedef struct {
     const double* d_y;      /* complex Y (per unit): [nnz] if y_shared else [n_scen][nnz] */

@@ -293,17 +293,18 @@ def flat_start(net: Network):
     return v
 
 
-def update_reference(bus_type, v, dx):
+def update_reference(bus_type, v, dx, damping=0.9):
     """update_voltage_estimates (cpu_newton_raphson.cpp:438-504): damping 0.9, |dtheta|
     clamp 0.15 rad, |d|V|| clamp 0.08, |V| clipped to [0.5, 1.5]; angles first (every
-    non-slack bus in bus order), then magnitudes (PQ buses in bus order)."""
+    non-slack bus in bus order), then magnitudes (PQ buses in bus order).  damping=1.0 is the
+    engine's 'clamped' policy (full step, same clamps)."""
     ang, mag, peq, qeq, ne = var_maps(bus_type)
     v = v.copy()
     n = len(v)
     for i in range(n):
         if ang[i] >= 0:
             vm = abs(v[i])
-            a = 0.9 * dx[ang[i]]
+            a = damping * dx[ang[i]]
             if abs(a) > 0.15:
                 a = 0.15 * (1.0 if a > 0 else -1.0)
             va = math.atan2(v[i].imag, v[i].real) + a
@@ -311,7 +312,7 @@ def update_reference(bus_type, v, dx):
     for i in range(n):
         if mag[i] >= 0:
             vm0 = abs(v[i])
-            c = 0.9 * dx[mag[i]]
+            c = damping * dx[mag[i]]
             if abs(c) > 0.08:
                 c = 0.08 * (1.0 if c > 0 else -1.0)
             vm = min(max(vm0 + c, 0.5), 1.5)
@@ -336,7 +337,8 @@ def nr_solve(net: Network, Y=None, tol=1e-8, max_iter=20, base_power=1e6,
              policy="reference", jac="reference", s_spec=None, v0=None, history=False):
     """CPUNewtonRaphson::solve_power_flow (cpu_newton_raphson.cpp:33-218) with a sparse LU.
 
-    policy 'reference' = the reference's damped, clamped update; 'newton' = pure Newton.
+    policy 'reference' = the reference's damped, clamped update; 'newton' = pure Newton;
+    'clamped' = full Newton step with the reference's clamps.
     jac 'reference' = last-wins duplicates and the 1e-12 drop; 'exact' = summed duplicates.
     Y defaults to the reference Y-bus (Siemens).  Returns dict(v, converged, iterations,
     final_mismatch[, trace])."""
@@ -370,7 +372,12 @@ def nr_solve(net: Network, Y=None, tol=1e-8, max_iter=20, base_power=1e6,
             # factorize() failed: the reference continues with zero corrections
             # (cpu_newton_raphson.cpp:416-419)
             dx = np.zeros(len(d))
-        v = update_reference(bt, v, dx) if policy == "reference" else update_newton(bt, v, dx)
+        if policy == "reference":
+            v = update_reference(bt, v, dx)
+        elif policy == "clamped":
+            v = update_reference(bt, v, dx, damping=1.0)
+        else:
+            v = update_newton(bt, v, dx)
     if not res["converged"]:
         res["iterations"] = max_iter
     res["v"] = v

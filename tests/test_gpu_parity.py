@@ -314,3 +314,36 @@ def test_sparse_lu_reference_unit_matrices_and_pivoting_cases():
     # numerically singular under static pivoting -> factorize reports failure
     rp, ci, va = _csr(np.array([[1, 1], [1, 1]], complex))
     assert not SparseLU(rp, ci).factorize(torch.as_tensor(va, device="cuda"))
+
+
+def test_clamped_policy_matches_oracle_from_flat_start():
+    """Full Newton steps with the reference's clamps, from the flat start (where the clamps
+    bind), against the oracle's same policy: same iteration count, voltages to 1e-8."""
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.transmission_grid(2, n=2000)
+    base = 1e8
+    zb = net.u_rated[0] ** 2 / base
+    S = 4
+    s_spec = synth.load_scenarios(net, S, sigma=0.1, seed=3, base_power=base)
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
+    b = NRBatch(plan, S, precision="fp64", lanes=4)
+    u = torch.as_tensor(net.u_pu.astype(np.float64), device="cuda")
+    r = b.solve(y, torch.as_tensor(s_spec, device="cuda"), u_pu=u, tol=1e-10, max_iter=40,
+                policy="clamped")
+    torch.cuda.synchronize()
+    assert (r.status.cpu().numpy() == 0).all()
+    V = r.v.cpu().numpy()
+    it = r.iterations.cpu().numpy()
+    Y = restate.ybus_pi(net)
+    for s in range(S):
+        o = restate.nr_solve(net, Y=Y, tol=1e-10, max_iter=40, base_power=base,
+                             policy="clamped", jac="exact", s_spec=s_spec[s])
+        assert o["converged"]
+        assert abs(int(it[s]) - o["iterations"]) <= 1
+        assert np.max(np.abs(V[s] - o["v"])) < 1e-8
