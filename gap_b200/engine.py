@@ -227,8 +227,9 @@ class NRBatch:
         return out
 
     # stage access (tests, profiling)
-    def stage_load(self, y, s_spec, v_init=None, u_pu=None, refine=0, stream=None):
-        inp = self._inputs(y, s_spec, v_init, u_pu, 0.0, 1, "newton", refine)
+    def stage_load(self, y, s_spec, v_init=None, u_pu=None, refine=0, stream=None,
+                   policy="newton"):
+        inp = self._inputs(y, s_spec, v_init, u_pu, 0.0, 1, policy, refine)
         N.check(N.lib().gapk_nr_stage_load(self._h, C.byref(inp), _stream_ptr(stream)))
 
     def stage(self, name, stream=None):
