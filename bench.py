@@ -177,7 +177,8 @@ class Clocks:
 # DRAM bytes per scenario per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
 # ncu --set full capture of the kernel on 256 scenarios of the same grid, scaled by scenarios
 # (each scenario's work and bytes are independent of the others).
-MEASURED_TRAFFIC_PER_SCENARIO = {"dense_lu": (966.46e6 + 1018.20e6) / 256}
+MEASURED_TRAFFIC_PER_SCENARIO = {"dense_lu": (855.51e6 + 950.34e6) / 256,
+                                 "schur": (116.22e6 + 180.02e6) / 256}
 
 
 def algorithmic_bytes(kernel, info, n_scen, esz):
