@@ -230,6 +230,38 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
             break;
     }
     if (dense_min <= 0 || T < dense_min) T = 0;
+    if (T > 0) {
+        // Extend the tail over the nodes just before it when that is cheaper: every extra
+        // node grows the dense LU (~N^3) and the dense solves (~N^2) but removes the outer
+        // products its column would add to the Schur gather (t_m^2 block pairs for a sparse
+        // node with t_m tail neighbours) -- the last sparse nodes before a min-degree tail are
+        // adjacent to most of it.  Costs per scenario in seconds, from B200 FP32 timings of
+        // the kernels: dense LU 2/3 N^3 flops at 18.5 TFLOP/s, 2.7 ps per Schur pair, two
+        // dense solves at 0.43 us per 466^2 entries.
+        const int T0 = T, ns0 = nb - T0;
+        const int kmax = std::min(ns0, 128);
+        auto cost = [&](int kk) {
+            const int nsk = ns0 - kk;
+            double pairs = 0.0;
+            for (int m = 0; m < nsk; ++m) {
+                const int* b = P.lidx.data() + P.lptr[m];
+                const int* e = P.lidx.data() + P.lptr[m + 1];
+                const double t = static_cast<double>(e - std::lower_bound(b, e, nsk));
+                pairs += t * t;
+            }
+            const double N = 2.0 * (T0 + kk);
+            return (2.0 / 3.0) * N * N * N / 18.5e12 + 2.72e-12 * pairs +
+                   8.6e-7 * (N / 466.0) * (N / 466.0);
+        };
+        double best = cost(0);
+        for (int kk = 4; kk <= kmax; kk += 4) {
+            const double c = cost(kk);
+            if (c < best) {
+                best = c;
+                T = T0 + kk;
+            }
+        }
+    }
     const int ns = nb - T;
     P.n_tail = T;
     P.ns = ns;
@@ -440,19 +472,29 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
         P.fb_ptr[h + 1] = static_cast<int>(P.scale.size() / 2);
     }
     // dense tail: (slot, pair_begin, pair_end, dense block position r*T + c)
+    // every one of the T^2 tail blocks gets a target, so the gather overwrites the whole
+    // dense block each iteration; blocks outside the symbolic structure (an extended tail is
+    // not full) have no pairs and no Jacobian value and are written as zero
     P.schur.clear();
     for (int k = ns; k < nb; ++k) {
         auto pe = emit(k);
         auto hs = [&](int sl) { return slot_a[sl] >= 0 ? (1 << 30) : 0; };
         P.schur.insert(P.schur.end(), {k, pe.first, pe.second, ((k - ns) * T + (k - ns)) | hs(k)});
-        for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
-            int a = P.lidx[p];
-            pe = emit(Ubase + p);
-            P.schur.insert(P.schur.end(), {Ubase + p, pe.first, pe.second,
-                                           ((k - ns) * T + (a - ns)) | hs(Ubase + p)});
-            pe = emit(Lbase + p);
-            P.schur.insert(P.schur.end(), {Lbase + p, pe.first, pe.second,
-                                           ((a - ns) * T + (k - ns)) | hs(Lbase + p)});
+        int p = P.lptr[k];
+        for (int a = k + 1; a < nb; ++a) {
+            if (p < P.lptr[k + 1] && P.lidx[p] == a) {
+                pe = emit(Ubase + p);
+                P.schur.insert(P.schur.end(), {Ubase + p, pe.first, pe.second,
+                                               ((k - ns) * T + (a - ns)) | hs(Ubase + p)});
+                pe = emit(Lbase + p);
+                P.schur.insert(P.schur.end(), {Lbase + p, pe.first, pe.second,
+                                               ((a - ns) * T + (k - ns)) | hs(Lbase + p)});
+                ++p;
+            } else {
+                const int pz = static_cast<int>(P.pairs.size() / 2);
+                P.schur.insert(P.schur.end(), {k, pz, pz, (k - ns) * T + (a - ns)});
+                P.schur.insert(P.schur.end(), {k, pz, pz, (a - ns) * T + (k - ns)});
+            }
         }
     }
 

@@ -63,7 +63,7 @@ def factor(plan, F):
         return F, None
     D = np.zeros((2 * T, 2 * T))
     for slot, pb, pe, pos in plan.export("schur").reshape(-1, 4):
-        acc = F[slot].copy()
+        acc = F[slot].copy() if (pos >> 30) & 1 else np.zeros((2, 2))
         for p in range(pb, pe):
             acc -= F[pr[p, 0]] @ F[pr[p, 1]]
         r, c = divmod(pos & ((1 << 30) - 1), T)
