@@ -474,26 +474,45 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
     // dense tail: (slot, pair_begin, pair_end, dense block position r*T + c)
     // every one of the T^2 tail blocks gets a target, so the gather overwrites the whole
     // dense block each iteration; blocks outside the symbolic structure (an extended tail is
-    // not full) have no pairs and no Jacobian value and are written as zero
-    P.schur.clear();
-    for (int k = ns; k < nb; ++k) {
-        auto pe = emit(k);
+    // not full) have no pairs and no Jacobian value and are written as zero.  Targets are in
+    // row-major block order: consecutive threads of one scenario write adjacent blocks.
+    P.schur.assign(static_cast<size_t>(T) * T * 4, 0);
+    {
         auto hs = [&](int sl) { return slot_a[sl] >= 0 ? (1 << 30) : 0; };
-        P.schur.insert(P.schur.end(), {k, pe.first, pe.second, ((k - ns) * T + (k - ns)) | hs(k)});
-        int p = P.lptr[k];
-        for (int a = k + 1; a < nb; ++a) {
-            if (p < P.lptr[k + 1] && P.lidx[p] == a) {
-                pe = emit(Ubase + p);
-                P.schur.insert(P.schur.end(), {Ubase + p, pe.first, pe.second,
-                                               ((k - ns) * T + (a - ns)) | hs(Ubase + p)});
-                pe = emit(Lbase + p);
-                P.schur.insert(P.schur.end(), {Lbase + p, pe.first, pe.second,
-                                               ((a - ns) * T + (k - ns)) | hs(Lbase + p)});
-                ++p;
+        auto put = [&](int r, int c, int slot, bool has) {
+            const size_t q = (static_cast<size_t>(r) * T + c) * 4;
+            if (has) {
+                auto pe = emit(slot);
+                P.schur[q] = slot;
+                P.schur[q + 1] = pe.first;
+                P.schur[q + 2] = pe.second;
+                P.schur[q + 3] = (r * T + c) | hs(slot);
             } else {
                 const int pz = static_cast<int>(P.pairs.size() / 2);
-                P.schur.insert(P.schur.end(), {k, pz, pz, (k - ns) * T + (a - ns)});
-                P.schur.insert(P.schur.end(), {k, pz, pz, (a - ns) * T + (k - ns)});
+                P.schur[q] = ns + r;
+                P.schur[q + 1] = pz;
+                P.schur[q + 2] = pz;
+                P.schur[q + 3] = r * T + c;
+            }
+        };
+        std::vector<int> ucol(T);
+        for (int r = 0; r < T; ++r) {
+            const int kr = ns + r;
+            // U(kr, a) for a > kr and L(a, kr): positions of row kr's column structure
+            std::fill(ucol.begin(), ucol.end(), -1);
+            for (int p = P.lptr[kr]; p < P.lptr[kr + 1]; ++p) ucol[P.lidx[p] - ns] = p;
+            for (int c = 0; c < T; ++c) {
+                if (c == r) {
+                    put(r, c, kr, true);
+                } else if (c > r) {
+                    const int p = ucol[c];
+                    put(r, c, p >= 0 ? Ubase + p : -1, p >= 0);
+                } else {
+                    // L(kr, ns + c) lives in column ns + c's structure
+                    const int kc = ns + c;
+                    const int p = find_in(P.lidx, P.lptr[kc], P.lptr[kc + 1], kr);
+                    put(r, c, p >= 0 ? Lbase + p : -1, p >= 0);
+                }
             }
         }
     }
