@@ -47,6 +47,8 @@ SIGMA = 0.1
 TOL = 1e-8
 MAX_ITER = 20
 BASE = 1e8
+# one FP64 refinement step per Newton correction once a lane group's max |mismatch| < 1e-4 pu
+REFINE_BELOW = 1e-4
 
 
 def workload(rank: int):
@@ -63,7 +65,8 @@ def workload(rank: int):
 def config(extra=None):
     c = {"workload": f"{N_SCEN} load scenarios x {N_BUS}-bus transmission grid (seed {GRID_SEED})",
          "n_bus": N_BUS, "scenarios_per_gpu": N_SCEN, "load_sigma": SIGMA, "tol_pu": TOL,
-         "max_iter": MAX_ITER, "precision": "fp32 factor+solve, fp64 mismatch/update, 1 refine",
+         "max_iter": MAX_ITER, "precision": "fp32 factor+solve, fp64 mismatch/update, 1 refine "
+                                                   "below 1e-4 pu",
          "policy": "newton", "start": "dc angles", "l2": "inputs larger than L2 (state > 300 MB)"}
     if extra:
         c.update(extra)
@@ -265,7 +268,7 @@ def run_ours(args, rank, world, device):
 
     def step():
         return batch.solve(y, s_dev, v_init=v_dev, tol=TOL, max_iter=MAX_ITER, policy="newton",
-                           refine=1)
+                           refine=1, refine_below=REFINE_BELOW)
 
     for _ in range(args.warmup):
         r = step()
@@ -299,7 +302,8 @@ def run_ours(args, rank, world, device):
     def e2e_step():
         sd = s_h.to("cuda", non_blocking=True)
         vd = v_h.to("cuda", non_blocking=True)
-        rr = batch.solve(y, sd, v_init=vd, tol=TOL, max_iter=MAX_ITER, policy="newton", refine=1)
+        rr = batch.solve(y, sd, v_init=vd, tol=TOL, max_iter=MAX_ITER, policy="newton", refine=1,
+                         refine_below=REFINE_BELOW)
         vo_h.copy_(rr.v, non_blocking=True)
         st_h.copy_(rr.status, non_blocking=True)
         it_h.copy_(rr.iterations, non_blocking=True)
@@ -482,7 +486,7 @@ def run_mixed(args):
                                         synth.dc_start(g, BASE), base_power=BASE))
     setup_s = time.perf_counter() - t0
     all_st = [load, cont] + grids
-    kw = dict(tol=TOL, max_iter=MAX_ITER, policy="newton", refine=1)
+    kw = dict(tol=TOL, max_iter=MAX_ITER, policy="newton", refine=1, refine_below=REFINE_BELOW)
     t1 = time.perf_counter()
     for st in all_st:
         studies.autotune(st, **kw)
@@ -519,7 +523,8 @@ def run_mixed(args):
                                "+ 64 independent grids, n log-uniform in [500, 20000]",
                    "grid_sizes": [int(g.net.n_bus) for g in grids],
                    "tol_pu": TOL, "max_iter": MAX_ITER, "policy": "newton",
-                   "precision": "fp32 factor+solve, fp64 mismatch/update, 1 refine",
+                   "precision": "fp32 factor+solve, fp64 mismatch/update, 1 refine "
+                                                   "below 1e-4 pu",
                    "streams": len(all_st), "autotuned_lanes_x_threads": picks,
                    "autotuned_load_and_n-1": [f"{st.lanes}x{st.threads}" for st in all_st[:2]]},
         "sequential_ms": seq, "concurrency_gain": seq / ms,
@@ -548,7 +553,7 @@ def run_large(args):
     b = st.make_batch()
     # full Newton steps with the reference's clamps: pure Newton diverges on a few of these
     # scenarios from the DC start (as the FP64 oracle does), the clamped steps converge
-    kw = dict(tol=TOL, max_iter=30, policy="clamped", refine=1)
+    kw = dict(tol=TOL, max_iter=30, policy="clamped", refine=1, refine_below=REFINE_BELOW)
     r = b.solve(st.y, st.s_spec, v_init=st.v0, **kw)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)

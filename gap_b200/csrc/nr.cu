@@ -152,7 +152,7 @@ struct gapk_nr_batch_s {
     gapk_nr_plan plan = nullptr;
     int n_scen = 0, sw = 8, G = 0, precision = 0, y_shared = 1, threads = 256, use_graph = 1;
     DevBuf V, Sspec, Scalc, Y, F, A64, rhs, dx, res, X, Dt, mis, state, solving, singular,
-        iters, status, fmis, gsolve, giter, ctrl, tol;
+        iters, status, fmis, gsolve, giter, grefine, ctrl, tol;
     int dense_w = 0;        // panel width of the dense-tail LU (0: no tail)
     size_t dense_smem = 0;  // dynamic shared memory of k_dense_lu
     BatchDev dev{};
@@ -177,7 +177,7 @@ template <typename T, int SW>
 void launch_solve(gapk_nr_batch b, cudaStream_t st, const double2* rhs, double2* out, int acc) {
     PlanDev const& P = b->plan->dev;
     BatchDev const& B = b->dev;
-    k_solve_fwd<T, SW><<<b->G, b->threads, 0, st>>>(P, B, rhs);
+    k_solve_fwd<T, SW><<<b->G, b->threads, 0, st>>>(P, B, rhs, acc);
     if (P.n_tail > 0)
         k_dense_solve<T, SW><<<b->G * SW, 256, 2 * P.n_tail * sizeof(T), st>>>(P, B, out, acc);
     k_solve_bwd<T, SW><<<b->G, b->threads, 0, st>>>(P, B, out, acc);
@@ -329,7 +329,7 @@ struct KernelOp {
                 if (P.n_tail > 0)
                     launch_dense_lu<T>(b->dense_w, G * SW, b->dense_smem, st, B, 2 * P.n_tail);
                 break;
-            case 5: k_solve_fwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs); break;
+            case 5: k_solve_fwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs, 0); break;
             case 6:
                 if (P.n_tail > 0)
                     k_dense_solve<T, SW><<<G * SW, 256, 2 * P.n_tail * sizeof(T), st>>>(P, B, B.dx, 0);
@@ -461,8 +461,12 @@ int load_inputs(gapk_nr_batch b, const gapk_nr_inputs* in, cudaStream_t st) {
     b->cur_refine = in->refine;
     int ctrl[5] = {0, in->max_iterations, 1, in->policy, 0};
     GAPK_CUDA_TRY(cudaMemcpyAsync(b->ctrl.p, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, st));
-    double tol = in->tolerance;
-    GAPK_CUDA_TRY(cudaMemcpyAsync(b->tol.p, &tol, sizeof(double), cudaMemcpyHostToDevice, st));
+    if (!(in->refine_below >= 0.0)) {
+        set_error("inputs: refine_below must be >= 0");
+        return GAPK_EINVAL;
+    }
+    double tol[2] = {in->tolerance, in->refine_below};
+    GAPK_CUDA_TRY(cudaMemcpyAsync(b->tol.p, tol, sizeof(tol), cudaMemcpyHostToDevice, st));
     dispatch_tsw<LoadOp>(b->precision, b->sw, b, in, st);
     return check_launch();
 }
@@ -674,7 +678,8 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     A(b->gsolve, G * 4);
     A(b->giter, G * 4);
     A(b->ctrl, 8 * 4);
-    A(b->tol, 8);
+    A(b->grefine, G * 4);
+    A(b->tol, 16);
     if (rc) return rc;
     BatchDev& d = b->dev;
     d.n_scen = n_scen;
@@ -703,6 +708,7 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     d.giter = b->giter.as<int>();
     d.ctrl = b->ctrl.as<int>();
     d.tol = b->tol.as<double>();
+    d.grefine = b->grefine.as<int>();
     *out = b.release();
     return GAPK_OK;
 }
@@ -717,7 +723,7 @@ int64_t gapk_nr_batch_device_bytes(gapk_nr_batch b) {
     int64_t s = 0;
     for (DevBuf* d : {&b->V, &b->Sspec, &b->Scalc, &b->Y, &b->F, &b->A64, &b->rhs, &b->dx,
                       &b->res, &b->X, &b->Dt, &b->mis, &b->state, &b->solving, &b->singular, &b->iters,
-                      &b->status, &b->fmis, &b->gsolve, &b->giter, &b->ctrl, &b->tol})
+                      &b->status, &b->fmis, &b->gsolve, &b->giter, &b->grefine, &b->ctrl, &b->tol})
         s += static_cast<int64_t>(d->bytes);
     return s;
 }
@@ -1181,7 +1187,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
             k_schur<double, 1><<<blocks_for((long)P.n_schur, 256), 256, 0, st>>>(P, D);
             launch_dense_lu<double>(dense_w, 1, dense_smem, st, D, (int)N);
         }
-        k_solve_fwd<double, 1><<<1, thr, 0, st>>>(P, D, D.rhs);
+        k_solve_fwd<double, 1><<<1, thr, 0, st>>>(P, D, D.rhs, 0);
         if (h.n_tail > 0)
             k_dense_solve<double, 1><<<1, 256, N * sizeof(double), st>>>(P, D, D.dx, 0);
         k_solve_bwd<double, 1><<<1, thr, 0, st>>>(P, D, D.dx, 0);

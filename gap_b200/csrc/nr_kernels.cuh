@@ -75,7 +75,8 @@ struct BatchDev {
     int* gsolve;      // [G]
     int* giter;       // [G]
     int* ctrl;        // [0] iteration, [1] max_iter, [2] any iterating, [3] policy, [4] loops
-    double* tol;      // [1]
+    double* tol;      // [0] tolerance, [1] refine below this mismatch (0: always); noalloc: [1] only tol
+    int* grefine;     // [G] refinement pass runs for the group this iteration (null: always)
 };
 
 // ---------------------------------------------------------------------------------------
@@ -124,6 +125,7 @@ __global__ void k_load(PlanDev P, BatchDev B, const double2* __restrict__ y_in,
         if (lane == 0) {
             B.gsolve[g] = 1;
             B.giter[g] = 1;
+            if (B.grefine) B.grefine[g] = 1;  // the stage API refines unless k_check says not
         }
     }
 }
@@ -238,6 +240,16 @@ __global__ void k_check(BatchDev B, int use_cond, cudaGraphConditionalHandle han
         }
         B.gsolve[g] = sv;
         B.giter[g] = iv;
+        if (B.grefine) {
+            // refinement only once some iterating lane of the group is close to convergence
+            const double rb = B.tol[1];
+            int rv = rb <= 0.0;
+            for (int l = 0; l < SW && !rv; ++l) {
+                const int q = g * SW + l;
+                if (q < B.n_scen && B.solving[q] && B.final_mis[q] < rb) rv = 1;
+            }
+            B.grefine[g] = rv;
+        }
         if (iv) atomicOr(&any_iter, 1);
     }
     __syncthreads();
@@ -726,6 +738,7 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
     const int q = blockIdx.x;
     if (q >= B.n_scen || !B.solving[q]) return;
     const int g = q / SW, lane = q % SW;
+    if (accumulate && B.grefine && !B.grefine[g]) return;
     const int N = 2 * P.n_tail, ld = dense_ld(N);
     const T* A = reinterpret_cast<const T*>(B.Dt) + (size_t)q * N * ld;
     Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
@@ -842,9 +855,10 @@ __device__ __forceinline__ Vec2<T> split_reduce(Vec2<T> acc, int s, int sub, int
 }
 
 template <typename T, int SW>
-__global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ rhs) {
+__global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ rhs,
+                            int refine_pass) {
     const int g = blockIdx.x;
-    if (!B.gsolve[g]) return;
+    if (!B.gsolve[g] || (refine_pass && B.grefine && !B.grefine[g])) return;
     __shared__ Vec2<T> red[256];  // (blockDim / (32 / SW)) partial sums, <= 256 for SW <= 8
     const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
     Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
@@ -900,7 +914,7 @@ __global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ r
 template <typename T, int SW>
 __global__ void k_solve_bwd(PlanDev P, BatchDev B, double2* out, int accumulate) {
     const int g = blockIdx.x;
-    if (!B.gsolve[g]) return;
+    if (!B.gsolve[g] || (accumulate && B.grefine && !B.grefine[g])) return;
     __shared__ Vec2<T> red[256];
     const Blk<T>* F = reinterpret_cast<const Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
     Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
@@ -958,7 +972,7 @@ __global__ void k_solve_bwd(PlanDev P, BatchDev B, double2* out, int accumulate)
 template <int SW>
 __global__ void __launch_bounds__(256) k_residual(PlanDev P, BatchDev B) {
     const int g = blockIdx.y;
-    if (!B.gsolve[g]) return;
+    if (!B.gsolve[g] || (B.grefine && !B.grefine[g])) return;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = tid / SW, lane = tid % SW;
     if (k >= P.nb) return;

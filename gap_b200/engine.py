@@ -201,17 +201,20 @@ class NRBatch:
     def device_bytes(self):
         return int(N.lib().gapk_nr_batch_device_bytes(self._h))
 
-    def _inputs(self, y, s_spec, v_init, u_pu, tol, max_iter, policy, refine):
+    def _inputs(self, y, s_spec, v_init, u_pu, tol, max_iter, policy, refine, refine_below=0.0):
         pol = {"reference": N.POLICY_REFERENCE, "newton": N.POLICY_NEWTON,
                "clamped": N.POLICY_CLAMPED}[policy]
         return N.Inputs(_dptr(y), _dptr(s_spec), _dptr(v_init), _dptr(u_pu), float(tol),
-                        int(max_iter), pol, int(refine))
+                        int(max_iter), pol, int(refine), float(refine_below))
 
     def solve(self, y, s_spec, v_init=None, u_pu=None, tol=1e-8, max_iter=20,
-              policy="reference", refine=0, out=None, stream=None) -> NRResult:
+              policy="reference", refine=0, out=None, stream=None,
+              refine_below=0.0) -> NRResult:
         """y: complex128 per-unit Y values, [nnz] (y_shared) or [S, nnz]; s_spec: complex128
         [S, n_bus]; v_init: complex128 [S, n_bus] or None (flat start); u_pu: float64
-        [n_bus] flat-start |V| of SLACK/PV buses."""
+        [n_bus] flat-start |V| of SLACK/PV buses.  refine_below > 0 runs the `refine`
+        refinement steps only in iterations where a scenario of the lane group has max
+        |mismatch| below it."""
         torch = _torch()
         n = self.plan.info["n_bus"]
         dev = s_spec.device
@@ -220,7 +223,7 @@ class NRBatch:
                            torch.empty(self.n_scen, dtype=torch.int32, device=dev),
                            torch.empty(self.n_scen, dtype=torch.int32, device=dev),
                            torch.empty(self.n_scen, dtype=torch.float64, device=dev))
-        inp = self._inputs(y, s_spec, v_init, u_pu, tol, max_iter, policy, refine)
+        inp = self._inputs(y, s_spec, v_init, u_pu, tol, max_iter, policy, refine, refine_below)
         o = N.Outputs(_dptr(out.v), _dptr(out.iterations), _dptr(out.status),
                       _dptr(out.final_mismatch))
         N.check(N.lib().gapk_nr_solve(self._h, C.byref(inp), C.byref(o), _stream_ptr(stream)))

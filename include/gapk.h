@@ -189,6 +189,9 @@ typedef struct {
     int max_iterations;
     int policy;             /* GAPK_POLICY_*                                                */
     int refine;             /* extra iterative-refinement steps on each Newton correction  */
+    double refine_below;    /* refine only in iterations where some iterating scenario of a
+                               lane group has max |mismatch| below this (0 = every iteration);
+                               far from the solution the FP32 step error does not slow Newton */
 } gapk_nr_inputs;
 
 typedef struct {

@@ -347,3 +347,40 @@ def test_clamped_policy_matches_oracle_from_flat_start():
         assert o["converged"]
         assert abs(int(it[s]) - o["iterations"]) <= 1
         assert np.max(np.abs(V[s] - o["v"])) < 1e-8
+
+
+def test_refinement_only_near_convergence_matches_oracle():
+    """FP32 factor with the refinement step run only once a group is near convergence
+    (refine_below): same converged voltages as the FP64 oracle, and refinement does run
+    (results differ from no refinement at all only through convergence, not accuracy)."""
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.transmission_grid(1, n=2000)
+    base = 1e8
+    zb = net.u_rated[0] ** 2 / base
+    S = 11
+    s_spec = synth.load_scenarios(net, S, sigma=0.1, seed=6, base_power=base)
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
+    b = NRBatch(plan, S, precision="fp32", lanes=4)
+    v0 = np.repeat(synth.dc_start(net, base)[None], S, axis=0)
+    s_t = torch.as_tensor(s_spec, device="cuda")
+    v_t = torch.as_tensor(v0, device="cuda")
+    r = b.solve(y, s_t, v_init=v_t, tol=1e-10, max_iter=30, policy="newton", refine=1,
+                refine_below=1e-4)
+    torch.cuda.synchronize()
+    assert (r.status.cpu().numpy() == 0).all()
+    V = r.v.cpu().numpy()
+    Y = restate.ybus_pi(net)
+    for s in (0, 5, 10):
+        o = restate.nr_solve(net, Y=Y, tol=1e-12, max_iter=30, base_power=base,
+                             policy="newton", jac="exact", s_spec=s_spec[s], v0=v0[s])
+        assert np.max(np.abs(np.abs(V[s]) - np.abs(o["v"]))) < 1e-8
+        assert np.max(np.abs(np.angle(V[s]) - np.angle(o["v"]))) < 1e-8
+    with pytest.raises(Exception):
+        b.solve(y, s_t, v_init=v_t, tol=1e-10, max_iter=30, policy="newton", refine=1,
+                refine_below=-1.0)
