@@ -153,8 +153,9 @@ struct gapk_nr_batch_s {
     int n_scen = 0, sw = 8, G = 0, precision = 0, y_shared = 1, threads = 256, use_graph = 1;
     DevBuf V, Sspec, Scalc, Y, F, A64, rhs, dx, res, X, Dt, mis, state, solving, singular,
         iters, status, fmis, gsolve, giter, grefine, ctrl, tol;
-    int dense_w = 0;        // panel width of the dense-tail LU (0: no tail)
-    size_t dense_smem = 0;  // dynamic shared memory of k_dense_lu
+    int dense_w = 0;          // panel width of the one-CTA-per-scenario dense LU (0: not used)
+    size_t dense_smem = 0;    // its dynamic shared memory
+    bool dense_split = false; // factorise the tail with the split kernels
     BatchDev dev{};
     // graph cache
     cudaGraph_t graph = nullptr;
@@ -191,7 +192,10 @@ void launch_factor(gapk_nr_batch b, cudaStream_t st) {
     if (P.n_tail > 0) {
         dim3 gs(blocks_for((long)P.n_schur * SW, 256), b->G);
         k_schur<T, SW><<<gs, 256, 0, st>>>(P, B);
-        launch_dense_lu<T>(b->dense_w, b->G * SW, b->dense_smem, st, B, 2 * P.n_tail);
+        if (b->dense_split)
+            launch_dense_lu_split<T>(b->G * SW, st, B, 2 * P.n_tail);
+        else
+            launch_dense_lu<T>(b->dense_w, b->G * SW, b->dense_smem, st, B, 2 * P.n_tail);
     }
 }
 
@@ -327,7 +331,10 @@ struct KernelOp {
                 break;
             case 4:
                 if (P.n_tail > 0)
-                    launch_dense_lu<T>(b->dense_w, G * SW, b->dense_smem, st, B, 2 * P.n_tail);
+                    if (b->dense_split)
+                        launch_dense_lu_split<T>(G * SW, st, B, 2 * P.n_tail);
+                    else
+                        launch_dense_lu<T>(b->dense_w, G * SW, b->dense_smem, st, B, 2 * P.n_tail);
                 break;
             case 5: k_solve_fwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs, 0); break;
             case 6:
@@ -643,6 +650,10 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     A(b->res, L * nb * 16);
     A(b->X, L * nb * 2 * esz);
     if (h.n_tail > 0) {
+        // Dense-tail LU: one CTA per scenario (k_dense_lu, the panel in shared memory) when
+        // there are enough scenarios to fill the GPU and the panel fits; otherwise the split
+        // kernels, which spread each scenario's trailing update over many CTAs and have no
+        // shared-memory limit on the tail size.
         const size_t N = 2 * (size_t)h.n_tail;
         const size_t smem_max = 232448 - 1024;  // opt-in shared memory per block, less static
         b->dense_w = 0;
@@ -654,18 +665,19 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
                 break;
             }
         }
-        if (b->dense_w == 0) {
-            set_error("dense tail of " + std::to_string(h.n_tail) +
-                      " nodes exceeds the shared-memory panel limit");
-            return GAPK_ERANGE;
-        }
+        int dev = 0, n_sm = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        b->dense_split = b->dense_w == 0 || L < 2 * (size_t)n_sm;
         A(b->Dt, L * N * dense_ld((int)N) * esz);
-        cudaError_t e = b->precision == GAPK_PREC_FP64
-                            ? dense_lu_attributes<double>(b->dense_w, b->dense_smem)
-                            : dense_lu_attributes<float>(b->dense_w, b->dense_smem);
-        if (e != cudaSuccess) {
-            set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-            return GAPK_ECUDA;
+        if (!b->dense_split) {
+            cudaError_t e = b->precision == GAPK_PREC_FP64
+                                ? dense_lu_attributes<double>(b->dense_w, b->dense_smem)
+                                : dense_lu_attributes<float>(b->dense_w, b->dense_smem);
+            if (e != cudaSuccess) {
+                set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+                return GAPK_ECUDA;
+            }
         }
     }
     A(b->mis, L * 8);

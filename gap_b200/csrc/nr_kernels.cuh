@@ -487,7 +487,8 @@ __host__ __device__ __forceinline__ size_t dense_lu_elems(int N, int W) {
 // A: factor the diagonal block A[k0.., k0..] (w <= W rows and columns) in the lanes of one warp.
 // Returns 1 if a pivot is below the tolerance.
 template <typename T, int W>
-__device__ __noinline__ int dense_diag_block(T* A, int ld, int k0, int w, T* PT, T* SL, T* SD) {
+__device__ __noinline__ int dense_diag_block(T* A, int ld, int k0, int w, T* PT, int pld, T* SL,
+                                             T* SD) {
     const int r = threadIdx.x & 31;
     T a[W];
     if (r < w) {
@@ -521,7 +522,7 @@ __device__ __noinline__ int dense_diag_block(T* A, int ld, int k0, int w, T* PT,
     }
     if (r < W) {
 #pragma unroll
-        for (int c = 0; c < W; ++c) PT[c * ld + r] = a[c];  // U11 read as PT[c][k], k <= c
+        for (int c = 0; c < W; ++c) PT[c * pld + r] = a[c];  // U11 read as PT[c][k], k <= c
     }
     if (r < w) {
         T* row = A + (size_t)(k0 + r) * ld + k0;
@@ -541,9 +542,10 @@ __device__ __noinline__ int dense_diag_block(T* A, int ld, int k0, int w, T* PT,
     return badl;
 }
 
-// B, one row of L21: x U11 = a for the row at `row` (W values), written back and to PT[c][r].
+// B, one row of L21: x U11 = a for the row at `row` (W values; U11 transposed in PT with row
+// stride pld), written back and, when PTr is given, to PTr[c * pld].
 template <typename T, int W>
-__device__ __noinline__ void dense_l21_row(T* row, const T* PT, const T* SD, T* PTr, int ld) {
+__device__ __noinline__ void dense_l21_row(T* row, const T* PT, int pld, const T* SD, T* PTr) {
     T x[W];
 #pragma unroll
     for (int c4 = 0; c4 < W; c4 += 4) {
@@ -556,7 +558,7 @@ __device__ __noinline__ void dense_l21_row(T* row, const T* PT, const T* SD, T* 
         T s0 = x[c], s1 = T(0);
 #pragma unroll
         for (int k4 = 0; k4 < c; k4 += 4) {
-            const V4<T> u = ld4(PT + c * ld + k4);
+            const V4<T> u = ld4(PT + c * pld + k4);
 #pragma unroll
             for (int t = 0; t < 4; ++t)
                 if (k4 + t < c) {
@@ -566,8 +568,10 @@ __device__ __noinline__ void dense_l21_row(T* row, const T* PT, const T* SD, T* 
         }
         x[c] = (s0 + s1) * SD[c];
     }
+    if (PTr) {
 #pragma unroll
-    for (int c = 0; c < W; ++c) PTr[c * ld] = x[c];
+        for (int c = 0; c < W; ++c) PTr[c * pld] = x[c];
+    }
 #pragma unroll
     for (int c4 = 0; c4 < W; c4 += 4) st4(row + c4, V4<T>{{x[c4], x[c4 + 1], x[c4 + 2], x[c4 + 3]}});
 }
@@ -621,7 +625,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchD
         const int n2 = m - w;  // > 0 only for full panels
         // ---- A: diagonal block, warp 0
         if (tid < 32) {
-            if (dense_diag_block<T, W>(A, ld, k0, w, PT, SL, SD)) bad = 1;
+            if (dense_diag_block<T, W>(A, ld, k0, w, PT, ld, SL, SD)) bad = 1;
         }
         __syncthreads();
         if (n2 > 0) {
@@ -629,7 +633,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchD
             for (int it = tid; it < 2 * n2; it += nt) {
                 if (it < n2) {
                     const int r = W + it;
-                    dense_l21_row<T, W>(A + (size_t)(k0 + r) * ld + k0, PT, SD, PT + r, ld);
+                    dense_l21_row<T, W>(A + (size_t)(k0 + r) * ld + k0, PT, ld, SD, PT + r);
                 } else {
                     dense_u12_col<T, W>(A + (size_t)k0 * ld + k0 + W + (it - n2), SL, ld);
                 }
@@ -650,7 +654,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchD
             stage(0, Ub0);
             cp_async_wait_all();
             __syncthreads();
-            const int tr = (n2 + 3) / 4;
             for (int ch = 0; ch < nch; ++ch) {
                 T* cur = (ch & 1) ? Ub1 : Ub0;
                 if (ch + 1 < nch) stage(ch + 1, (ch & 1) ? Ub0 : Ub1);
@@ -726,6 +729,136 @@ void launch_dense_lu(int W, int grid, size_t smem, cudaStream_t st, BatchDev con
         case 32: k_dense_lu<T, 32><<<grid, 256, smem, st>>>(B, N); break;
         case 16: k_dense_lu<T, 16><<<grid, 256, smem, st>>>(B, N); break;
         case 8: k_dense_lu<T, 8><<<grid, 256, smem, st>>>(B, N); break;
+    }
+}
+
+// Split dense LU (the batch path): the same right-looking factorisation as k_dense_lu, one
+// panel of W = 32 columns at a time, as two launches per panel so that the rank-W trailing
+// update of every scenario is spread over many small CTAs instead of one CTA per scenario:
+//   k_dlu_panel  one CTA per scenario: steps A and B (diagonal block in one warp, whole L21 rows
+//                and U12 columns per thread), written back to the tail in global memory;
+//   k_dlu_update one CTA per (scenario, 64 x 64 tile of the trailing matrix): the tile's L21
+//                rows (transposed) and U12 columns staged in shared memory, 8x8 register tiles
+//                per thread, C -= L21 U12 in place.
+// No dynamic shared memory, so the tail size is limited only by device memory.
+constexpr int DLU_W = 32, DLU_TILE = 64;
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_dlu_panel(BatchDev B, int N, int k0) {
+    constexpr int W = DLU_W;
+    const int q = blockIdx.x;
+    if (q >= B.n_scen || !B.solving[q]) return;
+    const int ld = dense_ld(N);
+    T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
+    __shared__ __align__(16) T U11[W * (W + 4)];  // transposed: U11[c][k], stride W + 4
+    __shared__ __align__(16) T SL[W * (W + 4)];   // L11 row-major, stride W + 4
+    __shared__ __align__(16) T SD[W];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int w = min(W, N - k0);
+    const int n2 = N - k0 - w;
+    if (tid < 32) {
+        if (dense_diag_block<T, W>(A, ld, k0, w, U11, W + 4, SL, SD)) B.singular[q] = 1;
+    }
+    __syncthreads();
+    for (int it = tid; it < 2 * n2; it += nt) {
+        if (it < n2)
+            dense_l21_row<T, W>(A + (size_t)(k0 + W + it) * ld + k0, U11, W + 4, SD, nullptr);
+        else
+            dense_u12_col<T, W>(A + (size_t)k0 * ld + k0 + W + (it - n2), SL, ld);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(64, sizeof(T) == 4 ? 8 : 4)
+    k_dlu_update(BatchDev B, int N, int k0, int tiles_j) {
+    constexpr int W = DLU_W, TS = DLU_TILE;
+    const int q = blockIdx.y;
+    if (q >= B.n_scen || !B.solving[q]) return;
+    const int ld = dense_ld(N);
+    T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
+    const int n2 = N - k0 - W;
+    const int i0 = (blockIdx.x / tiles_j) * TS, j0 = (blockIdx.x % tiles_j) * TS;
+    __shared__ __align__(16) T LT[W][TS];  // LT[c][r] = L21(i0 + r, c)
+    __shared__ __align__(16) T UT[W][TS];  // UT[r][c] = U12(r, j0 + c)
+    const int tid = threadIdx.x;
+    T* base = A + (size_t)(k0 + W) * ld + k0 + W;  // trailing matrix origin
+    {
+        // one L21 row per thread (TS rows, TS threads); rows past the matrix are zero
+        const int r = tid;
+        if (i0 + r < n2) {
+            const T* row = A + (size_t)(k0 + W + i0 + r) * ld + k0;
+#pragma unroll
+            for (int c4 = 0; c4 < W; c4 += 4) {
+                const V4<T> v = ld4(row + c4);
+#pragma unroll
+                for (int t = 0; t < 4; ++t) LT[c4 + t][r] = v.v[t];
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < W; ++c) LT[c][r] = T(0);
+        }
+        // U12 rows 0..W-1, columns j0..j0+TS-1 in groups of 4; a group that starts inside the
+        // matrix ends inside the padded row (k0 + W and ld are multiples of 8)
+        for (int e = tid; e < W * (TS / 4); e += TS) {
+            const int r2 = e / (TS / 4), c = (e % (TS / 4)) * 4;
+            const V4<T> v = j0 + c < n2 ? ld4(A + (size_t)(k0 + r2) * ld + k0 + W + j0 + c)
+                                        : V4<T>{{T(0), T(0), T(0), T(0)}};
+            st4(&UT[r2][c], v);
+        }
+    }
+    __syncthreads();
+    const int r0 = (tid / 8) * 8, c0 = (tid % 8) * 8;
+    if (i0 + r0 >= n2 || j0 + c0 >= n2) return;
+    T acc[8][8];
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) {
+        if (i0 + r0 + ii < n2) {
+            const T* row = base + (size_t)(i0 + r0 + ii) * ld + j0 + c0;
+            const V4<T> a = ld4(row), b = ld4(row + 4);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                acc[ii][c] = a.v[c];
+                acc[ii][c + 4] = b.v[c];
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc[ii][c] = T(0);
+        }
+    }
+#pragma unroll 2
+    for (int r = 0; r < W; ++r) {
+        const V4<T> l0 = ld4(&LT[r][r0]), l1 = ld4(&LT[r][r0 + 4]);
+        const V4<T> u0 = ld4(&UT[r][c0]), u1 = ld4(&UT[r][c0 + 4]);
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                acc[ii][c] = fma(-l0.v[ii], u0.v[c], acc[ii][c]);
+                acc[ii][c + 4] = fma(-l0.v[ii], u1.v[c], acc[ii][c + 4]);
+                acc[ii + 4][c] = fma(-l1.v[ii], u0.v[c], acc[ii + 4][c]);
+                acc[ii + 4][c + 4] = fma(-l1.v[ii], u1.v[c], acc[ii + 4][c + 4]);
+            }
+    }
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) {
+        if (i0 + r0 + ii < n2) {
+            T* row = base + (size_t)(i0 + r0 + ii) * ld + j0 + c0;
+            st4(row, V4<T>{{acc[ii][0], acc[ii][1], acc[ii][2], acc[ii][3]}});
+            st4(row + 4, V4<T>{{acc[ii][4], acc[ii][5], acc[ii][6], acc[ii][7]}});
+        }
+    }
+}
+
+// Host side: the split factorisation of every scenario's N x N tail (grid = padded scenarios).
+template <typename T>
+void launch_dense_lu_split(int grid, cudaStream_t st, BatchDev const& B, int N) {
+    for (int k0 = 0; k0 < N; k0 += DLU_W) {
+        k_dlu_panel<T><<<grid, 128, 0, st>>>(B, N, k0);
+        const int n2 = N - k0 - DLU_W;
+        if (n2 > 0) {
+            const int tj = (n2 + DLU_TILE - 1) / DLU_TILE;
+            k_dlu_update<T><<<dim3(tj * tj, grid), DLU_TILE, 0, st>>>(B, N, k0, tj);
+        }
     }
 }
 
