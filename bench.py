@@ -49,6 +49,8 @@ MAX_ITER = 20
 BASE = 1e8
 # one FP64 refinement step per Newton correction once a lane group's max |mismatch| < 1e-4 pu
 REFINE_BELOW = 1e-4
+# per-bus load scale of the large (100k-bus) workload
+LARGE_LOAD_SCALE = 0.025
 
 
 def workload(rank: int):
@@ -541,7 +543,9 @@ def run_large(args):
     from gap_b200 import studies, synth
 
     t0 = time.perf_counter()
-    net = synth.transmission_grid(GRID_SEED, n=args.large_buses)
+    # at 100k buses the headline's loading (p ~ U[0,1] x 0.05 pu) has no solution reachable
+    # from the DC start (FP64 and FP32 alike cycle at 4-11 pu); half of it converges
+    net = synth.transmission_grid(GRID_SEED, n=args.large_buses, load_scale=LARGE_LOAD_SCALE)
     v0 = synth.dc_start(net, BASE)
     S = 32
     s_load = synth.load_scenarios(net, S, sigma=SIGMA, seed=1, base_power=BASE)
@@ -576,7 +580,8 @@ def run_large(args):
         "higher_is_better": True, "dtype": "fp32+fp64",
         "data": "synthetic (seeded generator, no external dataset)",
         "config": {"workload": f"32 load scenarios x {args.large_buses}-bus transmission grid "
-                               f"(seed {GRID_SEED})", "policy": "clamped Newton",
+                               f"(seed {GRID_SEED}, load scale {LARGE_LOAD_SCALE})",
+                   "policy": "clamped Newton",
                    "max_iter": 30,
                    "n_tail": info["n_tail"], "nnz_l_blocks": info["nnz_l_blocks"],
                    "n_pairs": info["n_pairs"], "n_schur_pairs": info["n_schur_pairs"]},
