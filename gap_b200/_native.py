@@ -34,7 +34,7 @@ EXPORTS = [
     "gapk_nr_stage_factor", "gapk_nr_stage_solve", "gapk_nr_stage_get_correction",
     "gapk_nr_stage_get_mismatch", "gapk_nr_stage_kernel", "gapk_nr_solve_noalloc",
     "gapk_splu_create", "gapk_splu_destroy", "gapk_splu_size", "gapk_splu_factorize",
-    "gapk_splu_solve", "gapk_nr_adjoint", "gapk_nr_adjoint_branch",
+    "gapk_splu_solve", "gapk_nr_adjoint", "gapk_nr_adjoint_branch", "gapk_branch_flows",
 ]
 
 
@@ -93,6 +93,10 @@ def lib():
         L.gapk_ybus_assemble.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64,
                                          C.c_void_p, C.c_int64, C.c_int, C.c_double,
                                          C.c_void_p, C.c_int64, C.c_void_p]
+        L.gapk_branch_flows.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_int64, C.c_void_p, C.c_double,
+                                         C.c_double, C.c_void_p, C.c_void_p, C.c_int,
+                                         C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 

@@ -181,6 +181,55 @@ struct gapk_ybus_s {
     }
 };
 
+// Branch results of solved scenarios: thread per (scenario, branch).  The stamps are the
+// Y-bus builder's (same arithmetic, scaled to per unit), so the flows are those of the network
+// the Newton loop solved.  out[(s * m + j) * 9 ..] = p_from, q_from, i_from, s_from, p_to,
+// q_to, i_to, s_to, loading (W, var, A, VA); zeros for out-of-service branches (from < 0).
+__global__ void k_branch_flows(int n_scen, int n_bus, int m, const int* __restrict__ from,
+                               const int* __restrict__ to, const double* __restrict__ br,
+                               int64_t branch_stride, const double2* __restrict__ v, double zb,
+                               double base_power, double u_base, const double* __restrict__ i_n,
+                               const double* __restrict__ sn, int mode, double* __restrict__ out) {
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long)n_scen * m) return;
+    const int s = (int)(tid / m), j = (int)(tid % m);
+    double* o = out + (size_t)tid * 9;
+    const int f = from[j], t = to[j];
+    if (f < 0 || t < 0) {
+        for (int c = 0; c < 9; ++c) o[c] = 0.0;
+        return;
+    }
+    const Stamps st = branch_stamps(br + (size_t)s * branch_stride + (size_t)j * 6, mode);
+    const double2 vf = v[(size_t)s * n_bus + f], vt = v[(size_t)s * n_bus + t];
+    // currents into the branch at each end, per unit
+    const double ifr = zb * (st.ff.x * vf.x - st.ff.y * vf.y + st.ft.x * vt.x - st.ft.y * vt.y);
+    const double ifi = zb * (st.ff.x * vf.y + st.ff.y * vf.x + st.ft.x * vt.y + st.ft.y * vt.x);
+    const double itr = zb * (st.tf.x * vf.x - st.tf.y * vf.y + st.tt.x * vt.x - st.tt.y * vt.y);
+    const double iti = zb * (st.tf.x * vf.y + st.tf.y * vf.x + st.tt.x * vt.y + st.tt.y * vt.x);
+    // S = V conj(I), in VA
+    const double pf = (vf.x * ifr + vf.y * ifi) * base_power;
+    const double qf = (vf.y * ifr - vf.x * ifi) * base_power;
+    const double pt = (vt.x * itr + vt.y * iti) * base_power;
+    const double qt = (vt.y * itr - vt.x * iti) * base_power;
+    const double sf = hypot(pf, qf), stt = hypot(pt, qt);
+    const double k3 = 1.7320508075688772 * u_base;  // sqrt(3) x line-to-line base voltage
+    const double af = sf / (k3 * hypot(vf.x, vf.y)), at = stt / (k3 * hypot(vt.x, vt.y));
+    double load = 0.0;
+    if (i_n && i_n[j] > 0.0)
+        load = fmax(af, at) / i_n[j];
+    else if (sn && sn[j] > 0.0)
+        load = fmax(sf, stt) / sn[j];
+    o[0] = pf;
+    o[1] = qf;
+    o[2] = af;
+    o[3] = sf;
+    o[4] = pt;
+    o[5] = qt;
+    o[6] = at;
+    o[7] = stt;
+    o[8] = load;
+}
+
 extern "C" {
 
 int gapk_ybus_create(int n_bus, int n_branch, const int* h_from_idx, const int* h_to_idx,
@@ -255,6 +304,31 @@ int gapk_ybus_apply_changes(int n_changes, const int* d_pos, const double* d_par
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string("k_ybus_changes launch: ") + cudaGetErrorString(e));
+        return GAPK_ECUDA;
+    }
+    return GAPK_OK;
+}
+
+int gapk_branch_flows(int n_scen, int n_bus, int n_branch, const int* d_from, const int* d_to,
+                      const double* d_branch, int64_t branch_stride, const double* d_v,
+                      double base_power, double u_base, const double* d_i_n, const double* d_sn,
+                      int mode, double* d_out, void* stream) {
+    if (n_scen <= 0 || n_bus <= 0 || n_branch < 0 || base_power <= 0.0 || u_base <= 0.0 ||
+        (n_branch && (!d_from || !d_to || !d_branch || !d_v || !d_out)) || branch_stride < 0 ||
+        (n_scen > 1 && branch_stride != 0 && branch_stride < (int64_t)n_branch * 6) ||
+        (mode != GAPK_YBUS_REFERENCE && mode != GAPK_YBUS_TAPS)) {
+        set_error("gapk_branch_flows: bad arguments");
+        return GAPK_EINVAL;
+    }
+    if (n_branch == 0) return GAPK_OK;
+    const long total = (long)n_scen * n_branch;
+    const double zb = u_base * u_base / base_power;
+    k_branch_flows<<<(unsigned)((total + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        n_scen, n_bus, n_branch, d_from, d_to, d_branch, branch_stride,
+        reinterpret_cast<const double2*>(d_v), zb, base_power, u_base, d_i_n, d_sn, mode, d_out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("k_branch_flows launch: ") + cudaGetErrorString(e));
         return GAPK_ECUDA;
     }
     return GAPK_OK;

@@ -116,6 +116,36 @@ def shunt_params(net: Network) -> np.ndarray:
     return np.stack([np.asarray(g, np.float64), np.asarray(b, np.float64)], axis=1)
 
 
+BRANCH_RESULT_FIELDS = ("p_from", "q_from", "i_from", "s_from", "p_to", "q_to", "i_to", "s_to",
+                        "loading")
+
+
+def branch_flows(net: Network, v, base_power, taps=True, i_n=None, sn=None, branch=None,
+                 stream=None):
+    """Branch results on the device (gapk_branch_flows): v complex128 per-unit voltages
+    [S, n_bus] (cuda); branch (r1, x1, g1, b1, k, theta) [m, 6] or [S, m, 6] (cuda, default the
+    network's own).  Returns float64 [S, m, 9] in BRANCH_RESULT_FIELDS order (W, var, A, VA,
+    loading); out-of-service branches give zero rows."""
+    torch = _torch()
+    v = v.contiguous()
+    S = v.shape[0]
+    f, t, valid = net.branch_index()
+    dev = v.device
+    fi = torch.as_tensor(np.where(valid, f, -1).astype(np.int32), device=dev)
+    ti = torch.as_tensor(np.where(valid, t, -1).astype(np.int32), device=dev)
+    br = (torch.as_tensor(branch_params(net), device=dev) if branch is None else branch).contiguous()
+    bst = net.n_branch * 6 if br.dim() == 3 else 0
+    inn = None if i_n is None else torch.as_tensor(np.asarray(i_n, np.float64), device=dev)
+    snn = None if sn is None else torch.as_tensor(np.asarray(sn, np.float64), device=dev)
+    out = torch.zeros((S, net.n_branch, 9), dtype=torch.float64, device=dev)
+    N.check(N.lib().gapk_branch_flows(S, net.n_bus, net.n_branch, _dptr(fi), _dptr(ti),
+                                      _dptr(br), bst, _dptr(v), float(base_power),
+                                      float(net.u_rated[0]), _dptr(inn), _dptr(snn),
+                                      N.YBUS_TAPS if taps else N.YBUS_REFERENCE, _dptr(out),
+                                      _stream_ptr(stream)))
+    return out
+
+
 # ----------------------------------------------------------------------------------------
 # Newton-Raphson
 # ----------------------------------------------------------------------------------------

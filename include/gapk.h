@@ -101,6 +101,23 @@ int gapk_ybus_assemble(gapk_ybus y, int n_scen, const double* d_branch, int64_t 
 int gapk_ybus_apply_changes(int n_changes, const int* d_pos, const double* d_params,
                             double* d_values, void* stream);
 
+/* Branch results of solved scenarios: fills, per scenario and branch, the BranchData result
+ * fields p_from, q_from, i_from, s_from, p_to, q_to, i_to, s_to, loading
+ * (include/gap/core/types.h:233-243), which the reference declares but never computes; the
+ * definitions are power-grid-model's line outputs (W, var, A, VA; |I| = |S| / (sqrt(3)|U|);
+ * loading = max(i_from, i_to) / i_n, or max(s_from, s_to) / sn where i_n is absent or 0).
+ *   d_from, d_to : bus index per branch, -1 for an out-of-service branch (its row is zero)
+ *   d_branch     : (r1, x1, g1, b1, k, theta) per branch in Ohm / S, as gapk_ybus_assemble;
+ *                  branch_stride doubles between scenarios (0 = shared)
+ *   d_v          : complex per-unit voltages [n_scen][n_bus]; u_base the voltage base (V)
+ *   d_i_n, d_sn  : rated current (A) / power (VA) per branch, or NULL
+ *   mode         : GAPK_YBUS_REFERENCE (taps ignored, as the reference's Y-bus) or _TAPS
+ *   d_out        : [n_scen][n_branch][9] doubles */
+int gapk_branch_flows(int n_scen, int n_bus, int n_branch, const int* d_from, const int* d_to,
+                      const double* d_branch, int64_t branch_stride, const double* d_v,
+                      double base_power, double u_base, const double* d_i_n, const double* d_sn,
+                      int mode, double* d_out, void* stream);
+
 /* ==== Newton-Raphson engine ===========================================================
  * A plan holds everything that depends only on the Y pattern and the bus types: the
  * 2x2-block Jacobian pattern, a minimum-degree ordering, the symbolic block-LU

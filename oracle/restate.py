@@ -533,3 +533,39 @@ def ybus_update_reference(Y, changes: Network):
                     out[p] -= ys
                     break
     return row_ptr, col_idx, out
+
+
+def branch_flows(net: Network, v, base_power, i_n=None, sn=None, taps=True):
+    """Branch results of a solved network, in the units of the reference's BranchData result
+    fields (include/gap/core/types.h:233-243: p/q in W/var, s in VA, i in A, loading), which
+    the reference declares but never fills; definitions as power-grid-model's line output
+    (the reference's PGM validation data): S_from = V_f conj(I_f) with I_f = Y_ff V_f + Y_ft V_t
+    the current into the branch at its from end (pi model of the Y-bus builder), likewise at
+    the to end; |I| = |S| / (sqrt(3) |U|) with U the line-to-line voltage; loading =
+    max(i_from, i_to) / i_n, or max(s_from, s_to) / sn for a branch with sn > 0 and no i_n.
+    Returns ([m_in_service, 9] = p_from, q_from, i_from, s_from, p_to, q_to, i_to, s_to,
+    loading; the in-service branch indices)."""
+    zb = float(net.u_rated[0]) ** 2 / base_power
+    idx, f, t, y, yff, ytt, yft, ytf, tap = branch_stamps(net, zb, taps)
+    v = np.asarray(v, np.complex128)
+    vf, vt = v[f], v[t]
+    i_f = yff * vf + yft * vt
+    i_t = ytf * vf + ytt * vt
+    s_f = vf * np.conj(i_f) * base_power
+    s_t = vt * np.conj(i_t) * base_power
+    ub = float(net.u_rated[0])
+    sq3 = math.sqrt(3.0)
+    a_f = np.abs(s_f) / (sq3 * np.abs(vf) * ub)
+    a_t = np.abs(s_t) / (sq3 * np.abs(vt) * ub)
+    load = np.zeros(len(idx))
+    if i_n is not None:
+        inn = np.asarray(i_n, np.float64)[idx] if len(i_n) == net.n_branch else np.asarray(i_n)
+        load = np.where(inn > 0, np.maximum(a_f, a_t) / np.where(inn > 0, inn, 1.0), 0.0)
+    if sn is not None:
+        snn = np.asarray(sn, np.float64)[idx] if len(sn) == net.n_branch else np.asarray(sn)
+        use = (snn > 0) & (load == 0)
+        load = np.where(use, np.maximum(np.abs(s_f), np.abs(s_t)) / np.where(snn > 0, snn, 1.0),
+                        load)
+    out = np.stack([s_f.real, s_f.imag, a_f, np.abs(s_f), s_t.real, s_t.imag, a_t, np.abs(s_t),
+                    load], axis=1)
+    return out, idx

@@ -108,9 +108,19 @@ def make_pgm(ref_root):
                                     float(net.x_pu[i]) * zb, float(net.b_pu[i]) / zb, 1])
         gnet = simple_lists_to_network(bus_data, branch_data)
         sol = ref_all(gnet, 1e-8, 20, net.base_power)
+        # power-grid-model's line results, in branch_data order (in-service branches), and the
+        # lines' rated currents from the input: the branch-flow golden vectors
+        lines_out = {ln["id"]: ln for ln in ref.get("line", [])}
+        lines_in = {ln["id"]: ln for ln in json.load(open(inp))["data"].get("line", [])}
+        keys = ("p_from", "q_from", "i_from", "s_from", "p_to", "q_to", "i_to", "s_to", "loading")
+        bids = [int(b[0]) for b in branch_data]
+        extra = {}
+        if bids and all(b in lines_out and b in lines_in for b in bids):
+            extra["pgm_line"] = np.array([[float(lines_out[b][kk]) for kk in keys] for b in bids])
+            extra["pgm_line_i_n"] = np.array([float(lines_in[b]["i_n"]) for b in bids])
         save("pgm_" + case, bus_data=np.asarray(bus_data), branch_data=np.asarray(branch_data),
              base_power=np.float64(net.base_power), pgm_u_pu=pgm_u, pgm_u_angle=pgm_a,
-             **sol)
+             **sol, **extra)
         made.append(case)
     return made
 
