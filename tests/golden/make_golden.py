@@ -66,6 +66,9 @@ def simple_lists_to_network(bus_data, branch_data):
                          to_id=br[:, 2].astype(int), r1=br[:, 3], x1=br[:, 4], b1=b1)
 
 
+PGM_JSON_CASES = ("radial_1feeder_2nodepf", "radial_2feeder_8nodepf", "radial_3feeder_8nodepf")
+
+
 def make_pgm(ref_root):
     sys.path.insert(0, os.path.join(ref_root, "tests", "pgm_validation"))
     from json_io.gap_json_parser import PGMJSONParser  # reference code, used only here
@@ -118,6 +121,12 @@ def make_pgm(ref_root):
         if bids and all(b in lines_out and b in lines_in for b in bids):
             extra["pgm_line"] = np.array([[float(lines_out[b][kk]) for kk in keys] for b in bids])
             extra["pgm_line_i_n"] = np.array([float(lines_in[b]["i_n"]) for b in bids])
+        if case in PGM_JSON_CASES:
+            # the PGM input itself (zlib-compressed JSON text), for the PGM reader's tests
+            import zlib
+
+            extra["pgm_input_json_z"] = np.frombuffer(zlib.compress(open(inp, "rb").read(), 9),
+                                                      np.uint8)
         save("pgm_" + case, bus_data=np.asarray(bus_data), branch_data=np.asarray(branch_data),
              base_power=np.float64(net.base_power), pgm_u_pu=pgm_u, pgm_u_angle=pgm_a,
              **sol, **extra)
