@@ -344,7 +344,9 @@ __global__ void __launch_bounds__(256) k_jfill(PlanDev P, BatchDev B) {
     }
     Blk<T>* F = reinterpret_cast<Blk<T>*>(B.F) + ((size_t)g * P.n_slots + slot) * SW + lane;
     stb(F, Blk<T>{(T)J.a, (T)J.b, (T)J.c, (T)J.d});
-    if (B.A64) {
+    // the FP64 copy feeds only the refinement residual: skipped for groups that do not
+    // refine this iteration
+    if (B.A64 && (!B.grefine || B.grefine[g])) {
         Blk<double>* A = reinterpret_cast<Blk<double>*>(B.A64) +
                          ((size_t)g * P.n_a + a_idx) * SW + lane;
         stb(A, J);
