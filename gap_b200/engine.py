@@ -306,6 +306,51 @@ class NRBatch:
             pass
 
 
+class HostPipeline:
+    """Batched solves from and to host memory with the copies overlapped: the scenarios are
+    split into `chunks` contiguous parts (multiples of the lane count), each with its own
+    NRBatch and CUDA stream, so the device solves one part while the next part's inputs and the
+    previous part's results cross PCIe.  Host tensors should be pinned for the copies to be
+    asynchronous."""
+
+    def __init__(self, plan: NRPlan, n_scen: int, chunks=2, precision="fp32", lanes=8,
+                 threads=1024):
+        torch = _torch()
+        require_cuda()
+        n_scen = int(n_scen)
+        chunks = max(1, min(int(chunks), n_scen))
+        step = -(-n_scen // chunks)
+        step = -(-step // max(1, lanes)) * max(1, lanes)
+        self.ranges = [(a, min(a + step, n_scen)) for a in range(0, n_scen, step)]
+        self.batches = [NRBatch(plan, b - a, precision=precision, lanes=lanes, threads=threads)
+                        for a, b in self.ranges]
+        self.streams = [torch.cuda.Stream() for _ in self.ranges]
+        self.plan = plan
+        self.n_scen = n_scen
+
+    def solve(self, y, s_host, v_host, out_v, out_status=None, out_iterations=None,
+              out_mismatch=None, **kw):
+        """y: device per-unit Y [nnz]; s_host, v_host: host complex128 [S, n_bus]; results
+        into the host tensors out_v [S, n_bus] (and optionally status, iterations, final
+        mismatch [S]).  Returns after every part's results are on the host."""
+        torch = _torch()
+        cur = torch.cuda.current_stream()
+        for st in self.streams:
+            st.wait_stream(cur)
+        for (a, b), bt, st in zip(self.ranges, self.batches, self.streams):
+            with torch.cuda.stream(st):
+                sd = s_host[a:b].to("cuda", non_blocking=True)
+                vd = v_host[a:b].to("cuda", non_blocking=True)
+                r = bt.solve(y, sd, v_init=vd, stream=st, **kw)
+                out_v[a:b].copy_(r.v, non_blocking=True)
+                for host, dev in ((out_status, r.status), (out_iterations, r.iterations),
+                                  (out_mismatch, r.final_mismatch)):
+                    if host is not None:
+                        host[a:b].copy_(dev, non_blocking=True)
+        for st in self.streams:
+            st.synchronize()
+
+
 # ----------------------------------------------------------------------------------------
 # General sparse LU
 # ----------------------------------------------------------------------------------------

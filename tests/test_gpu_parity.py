@@ -421,3 +421,39 @@ def test_dense_tail_paths_agree():
         o = restate.nr_solve(net, Y=Y, tol=1e-12, max_iter=30, base_power=base,
                              policy="newton", jac="exact", s_spec=s_spec[s], v0=v0[s])
         assert np.max(np.abs(Vb[s] - o["v"])) < 1e-8
+
+
+def test_host_pipeline_equals_one_batch():
+    """Solving from pinned host buffers in two stream-overlapped parts gives bit-identical
+    results to one device batch (the parts keep the lane groups)."""
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import HostPipeline, NRBatch, NRPlan, YbusPlan, branch_params, \
+        shunt_params
+
+    net = synth.transmission_grid(5, n=1200)
+    base = 1e8
+    zb = net.u_rated[0] ** 2 / base
+    S = 48
+    s_spec = synth.load_scenarios(net, S, sigma=0.1, seed=4, base_power=base)
+    v0 = np.repeat(synth.dc_start(net, base)[None], S, axis=0)
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
+    kw = dict(tol=1e-10, max_iter=30, policy="newton", refine=1, refine_below=1e-4)
+    one = NRBatch(plan, S, precision="fp32", lanes=8, threads=1024).solve(
+        y, torch.as_tensor(s_spec, device="cuda"), v_init=torch.as_tensor(v0, device="cuda"),
+        **kw)
+    s_h = torch.as_tensor(s_spec).pin_memory()
+    v_h = torch.as_tensor(v0).pin_memory()
+    vo = torch.empty((S, net.n_bus), dtype=torch.complex128).pin_memory()
+    st = torch.empty(S, dtype=torch.int32).pin_memory()
+    it = torch.empty(S, dtype=torch.int32).pin_memory()
+    pipe = HostPipeline(plan, S, chunks=2, precision="fp32", lanes=8)
+    assert pipe.ranges == [(0, 24), (24, 48)]
+    for _ in range(2):
+        pipe.solve(y, s_h, v_h, vo, st, it, **kw)
+        assert torch.equal(vo, one.v.cpu())
+        assert torch.equal(st, one.status.cpu()) and (st.numpy() == 0).all()
+        assert torch.equal(it, one.iterations.cpu())
