@@ -49,6 +49,8 @@ MAX_ITER = 20
 BASE = 1e8
 # one FP64 refinement step per Newton correction once a lane group's max |mismatch| < 1e-4 pu
 REFINE_BELOW = 1e-4
+# ... and below the same mismatch the lane group keeps its previous LU factors
+REUSE_BELOW = 1e-4
 # per-bus load scale of the large (100k-bus) workload
 LARGE_LOAD_SCALE = 0.025
 
@@ -67,8 +69,8 @@ def workload(rank: int):
 def config(extra=None):
     c = {"workload": f"{N_SCEN} load scenarios x {N_BUS}-bus transmission grid (seed {GRID_SEED})",
          "n_bus": N_BUS, "scenarios_per_gpu": N_SCEN, "load_sigma": SIGMA, "tol_pu": TOL,
-         "max_iter": MAX_ITER, "precision": "fp32 factor+solve, fp64 mismatch/update, 1 refine "
-                                                   "below 1e-4 pu",
+         "max_iter": MAX_ITER, "precision": "fp32 factor+solve, fp64 mismatch/update; below 1e-4 pu: 1 "
+                                                   "refine, factors reused",
          "policy": "newton", "start": "dc angles", "l2": "inputs larger than L2 (state > 300 MB)"}
     if extra:
         c.update(extra)
@@ -272,7 +274,7 @@ def run_ours(args, rank, world, device):
 
     def step():
         return batch.solve(y, s_dev, v_init=v_dev, tol=TOL, max_iter=MAX_ITER, policy="newton",
-                           refine=1, refine_below=REFINE_BELOW)
+                           refine=1, refine_below=REFINE_BELOW, reuse_below=REUSE_BELOW)
 
     for _ in range(args.warmup):
         r = step()
@@ -308,7 +310,8 @@ def run_ours(args, rank, world, device):
 
     def e2e_step():
         pipe.solve(y, s_h, v_h, vo_h, st_h, it_h, fm_h, tol=TOL, max_iter=MAX_ITER,
-                   policy="newton", refine=1, refine_below=REFINE_BELOW)
+                   policy="newton", refine=1, refine_below=REFINE_BELOW,
+                   reuse_below=REUSE_BELOW)
 
     e2e_step()
     torch.cuda.synchronize()
@@ -488,7 +491,8 @@ def run_mixed(args):
                                         synth.dc_start(g, BASE), base_power=BASE))
     setup_s = time.perf_counter() - t0
     all_st = [load, cont] + grids
-    kw = dict(tol=TOL, max_iter=MAX_ITER, policy="newton", refine=1, refine_below=REFINE_BELOW)
+    kw = dict(tol=TOL, max_iter=MAX_ITER, policy="newton", refine=1, refine_below=REFINE_BELOW,
+              reuse_below=REUSE_BELOW)
     t1 = time.perf_counter()
     for st in all_st:
         studies.autotune(st, **kw)
@@ -525,8 +529,8 @@ def run_mixed(args):
                                "+ 64 independent grids, n log-uniform in [500, 20000]",
                    "grid_sizes": [int(g.net.n_bus) for g in grids],
                    "tol_pu": TOL, "max_iter": MAX_ITER, "policy": "newton",
-                   "precision": "fp32 factor+solve, fp64 mismatch/update, 1 refine "
-                                                   "below 1e-4 pu",
+                   "precision": "fp32 factor+solve, fp64 mismatch/update; below 1e-4 pu: 1 "
+                                                   "refine, factors reused",
                    "streams": len(all_st), "autotuned_lanes_x_threads": picks,
                    "autotuned_load_and_n-1": [f"{st.lanes}x{st.threads}" for st in all_st[:2]]},
         "sequential_ms": seq, "concurrency_gain": seq / ms,
@@ -557,7 +561,8 @@ def run_large(args):
     b = st.make_batch()
     # full Newton steps with the reference's clamps: pure Newton diverges on a few of these
     # scenarios from the DC start (as the FP64 oracle does), the clamped steps converge
-    kw = dict(tol=TOL, max_iter=30, policy="clamped", refine=1, refine_below=REFINE_BELOW)
+    kw = dict(tol=TOL, max_iter=30, policy="clamped", refine=1, refine_below=REFINE_BELOW,
+              reuse_below=REUSE_BELOW)
     r = b.solve(st.y, st.s_spec, v_init=st.v0, **kw)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)

@@ -152,7 +152,7 @@ struct gapk_nr_batch_s {
     gapk_nr_plan plan = nullptr;
     int n_scen = 0, sw = 8, G = 0, precision = 0, y_shared = 1, threads = 256, use_graph = 1;
     DevBuf V, Sspec, Scalc, Y, F, A64, rhs, dx, res, X, Dt, mis, state, solving, singular,
-        iters, status, fmis, gsolve, giter, grefine, ctrl, tol;
+        iters, status, fmis, gsolve, giter, grefine, gfactor, ctrl, tol;
     int dense_w = 0;          // panel width of the one-CTA-per-scenario dense LU (0: not used)
     size_t dense_smem = 0;    // its dynamic shared memory
     bool dense_split = false; // factorise the tail with the split kernels
@@ -468,11 +468,15 @@ int load_inputs(gapk_nr_batch b, const gapk_nr_inputs* in, cudaStream_t st) {
     b->cur_refine = in->refine;
     int ctrl[5] = {0, in->max_iterations, 1, in->policy, 0};
     GAPK_CUDA_TRY(cudaMemcpyAsync(b->ctrl.p, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, st));
-    if (!(in->refine_below >= 0.0)) {
-        set_error("inputs: refine_below must be >= 0");
+    if (!(in->refine_below >= 0.0) || !(in->reuse_below >= 0.0)) {
+        set_error("inputs: refine_below and reuse_below must be >= 0");
         return GAPK_EINVAL;
     }
-    double tol[2] = {in->tolerance, in->refine_below};
+    if (in->reuse_below > 0.0 && in->refine < 1) {
+        set_error("inputs: reuse_below > 0 needs refine >= 1");
+        return GAPK_EINVAL;
+    }
+    double tol[3] = {in->tolerance, in->refine_below, in->reuse_below};
     GAPK_CUDA_TRY(cudaMemcpyAsync(b->tol.p, tol, sizeof(tol), cudaMemcpyHostToDevice, st));
     dispatch_tsw<LoadOp>(b->precision, b->sw, b, in, st);
     return check_launch();
@@ -691,8 +695,13 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     A(b->giter, G * 4);
     A(b->ctrl, 8 * 4);
     A(b->grefine, G * 4);
-    A(b->tol, 16);
+    A(b->gfactor, G * 4);
+    A(b->tol, 24);
     if (rc) return rc;
+    // per-group flags start true (any non-zero byte pattern): callers that factorise without
+    // a load (the general LU) refine and refactorise as before
+    GAPK_CUDA_TRY(cudaMemset(b->grefine.p, 1, b->grefine.bytes));
+    GAPK_CUDA_TRY(cudaMemset(b->gfactor.p, 1, b->gfactor.bytes));
     BatchDev& d = b->dev;
     d.n_scen = n_scen;
     d.n_groups = b->G;
@@ -721,6 +730,7 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     d.ctrl = b->ctrl.as<int>();
     d.tol = b->tol.as<double>();
     d.grefine = b->grefine.as<int>();
+    d.gfactor = b->gfactor.as<int>();
     *out = b.release();
     return GAPK_OK;
 }
@@ -735,7 +745,7 @@ int64_t gapk_nr_batch_device_bytes(gapk_nr_batch b) {
     int64_t s = 0;
     for (DevBuf* d : {&b->V, &b->Sspec, &b->Scalc, &b->Y, &b->F, &b->A64, &b->rhs, &b->dx,
                       &b->res, &b->X, &b->Dt, &b->mis, &b->state, &b->solving, &b->singular, &b->iters,
-                      &b->status, &b->fmis, &b->gsolve, &b->giter, &b->grefine, &b->ctrl, &b->tol})
+                      &b->status, &b->fmis, &b->gsolve, &b->giter, &b->grefine, &b->gfactor, &b->ctrl, &b->tol})
         s += static_cast<int64_t>(d->bytes);
     return s;
 }

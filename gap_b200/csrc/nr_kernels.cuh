@@ -75,8 +75,11 @@ struct BatchDev {
     int* gsolve;      // [G]
     int* giter;       // [G]
     int* ctrl;        // [0] iteration, [1] max_iter, [2] any iterating, [3] policy, [4] loops
-    double* tol;      // [0] tolerance, [1] refine below this mismatch (0: always); noalloc: [1] only tol
+    double* tol;      // [0] tolerance, [1] refine below, [2] reuse the factors below this mismatch
+                      //     (0: never); the allocation-free path has [0] only
     int* grefine;     // [G] refinement pass runs for the group this iteration (null: always)
+    int* gfactor;     // [G] the group refactorises this iteration (null: always); else the
+                      //     previous factors precondition the refined solve
 };
 
 // ---------------------------------------------------------------------------------------
@@ -126,6 +129,7 @@ __global__ void k_load(PlanDev P, BatchDev B, const double2* __restrict__ y_in,
             B.gsolve[g] = 1;
             B.giter[g] = 1;
             if (B.grefine) B.grefine[g] = 1;  // the stage API refines unless k_check says not
+            if (B.gfactor) B.gfactor[g] = 1;
         }
     }
 }
@@ -248,7 +252,19 @@ __global__ void k_check(BatchDev B, int use_cond, cudaGraphConditionalHandle han
                 const int q = g * SW + l;
                 if (q < B.n_scen && B.solving[q] && B.final_mis[q] < rb) rv = 1;
             }
-            B.grefine[g] = rv;
+            // the factors are reused once every iterating lane of the group is below [2];
+            // the solve is then refined against the current FP64 Jacobian
+            const double rf = B.tol[2];
+            int fv = 1;
+            if (B.gfactor && rf > 0.0 && sv) {
+                fv = 0;
+                for (int l = 0; l < SW; ++l) {
+                    const int q = g * SW + l;
+                    if (q < B.n_scen && B.solving[q] && !(B.final_mis[q] < rf)) fv = 1;
+                }
+            }
+            if (B.gfactor) B.gfactor[g] = fv;
+            B.grefine[g] = rv || !fv;
         }
         if (iv) atomicOr(&any_iter, 1);
     }
@@ -342,8 +358,10 @@ __global__ void __launch_bounds__(256) k_jfill(PlanDev P, BatchDev B) {
         if (fabs(J.c) <= 1e-12) J.c = 0.0;
         if (fabs(J.d) <= 1e-12 && !(diag && J.d == 1.0)) J.d = 0.0;
     }
-    Blk<T>* F = reinterpret_cast<Blk<T>*>(B.F) + ((size_t)g * P.n_slots + slot) * SW + lane;
-    stb(F, Blk<T>{(T)J.a, (T)J.b, (T)J.c, (T)J.d});
+    if (!B.gfactor || B.gfactor[g]) {  // a group that reuses its factors keeps them
+        Blk<T>* F = reinterpret_cast<Blk<T>*>(B.F) + ((size_t)g * P.n_slots + slot) * SW + lane;
+        stb(F, Blk<T>{(T)J.a, (T)J.b, (T)J.c, (T)J.d});
+    }
     // the FP64 copy feeds only the refinement residual: skipped for groups that do not
     // refine this iteration
     if (B.A64 && (!B.grefine || B.grefine[g])) {
@@ -359,7 +377,7 @@ __global__ void __launch_bounds__(256) k_jfill(PlanDev P, BatchDev B) {
 template <typename T, int SW>
 __global__ void k_factor(PlanDev P, BatchDev B) {
     const int g = blockIdx.x;
-    if (!B.gsolve[g]) return;
+    if (!B.gsolve[g] || (B.gfactor && !B.gfactor[g])) return;
     Blk<T>* F = reinterpret_cast<Blk<T>*>(B.F) + (size_t)g * P.n_slots * SW;
     const int lane = threadIdx.x % SW;
     const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
@@ -426,7 +444,7 @@ __device__ __forceinline__ void st4(double* p, V4<double> const& a) {
 template <typename T, int SW>
 __global__ void __launch_bounds__(256) k_schur(PlanDev P, BatchDev B) {
     const int g = blockIdx.y;
-    if (!B.gsolve[g]) return;
+    if (!B.gsolve[g] || (B.gfactor && !B.gfactor[g])) return;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int t = tid / SW, lane = tid % SW;
     if (t >= P.n_schur) return;
@@ -608,7 +626,7 @@ template <typename T, int W>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchDev B, int N) {
     static_assert(W == 8 || W == 16 || W == 32, "panel width");
     const int q = blockIdx.x;
-    if (q >= B.n_scen || !B.solving[q]) return;
+    if (q >= B.n_scen || !B.solving[q] || (B.gfactor && !B.gfactor[q / B.sw])) return;
     const int ld = dense_ld(N);
     T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -749,7 +767,7 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_dlu_panel(BatchDev B, int N, int k0) {
     constexpr int W = DLU_W;
     const int q = blockIdx.x;
-    if (q >= B.n_scen || !B.solving[q]) return;
+    if (q >= B.n_scen || !B.solving[q] || (B.gfactor && !B.gfactor[q / B.sw])) return;
     const int ld = dense_ld(N);
     T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
     __shared__ __align__(16) T U11[W * (W + 4)];  // transposed: U11[c][k], stride W + 4
@@ -775,7 +793,7 @@ __global__ void __launch_bounds__(64, sizeof(T) == 4 ? 8 : 4)
     k_dlu_update(BatchDev B, int N, int k0, int tiles_j) {
     constexpr int W = DLU_W, TS = DLU_TILE;
     const int q = blockIdx.y;
-    if (q >= B.n_scen || !B.solving[q]) return;
+    if (q >= B.n_scen || !B.solving[q] || (B.gfactor && !B.gfactor[q / B.sw])) return;
     const int ld = dense_ld(N);
     T* A = reinterpret_cast<T*>(B.Dt) + (size_t)q * N * ld;
     const int n2 = N - k0 - W;

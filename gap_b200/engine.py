@@ -231,20 +231,24 @@ class NRBatch:
     def device_bytes(self):
         return int(N.lib().gapk_nr_batch_device_bytes(self._h))
 
-    def _inputs(self, y, s_spec, v_init, u_pu, tol, max_iter, policy, refine, refine_below=0.0):
+    def _inputs(self, y, s_spec, v_init, u_pu, tol, max_iter, policy, refine, refine_below=0.0,
+                reuse_below=0.0):
         pol = {"reference": N.POLICY_REFERENCE, "newton": N.POLICY_NEWTON,
                "clamped": N.POLICY_CLAMPED}[policy]
         return N.Inputs(_dptr(y), _dptr(s_spec), _dptr(v_init), _dptr(u_pu), float(tol),
-                        int(max_iter), pol, int(refine), float(refine_below))
+                        int(max_iter), pol, int(refine), float(refine_below),
+                        float(reuse_below))
 
     def solve(self, y, s_spec, v_init=None, u_pu=None, tol=1e-8, max_iter=20,
               policy="reference", refine=0, out=None, stream=None,
-              refine_below=0.0) -> NRResult:
+              refine_below=0.0, reuse_below=0.0) -> NRResult:
         """y: complex128 per-unit Y values, [nnz] (y_shared) or [S, nnz]; s_spec: complex128
         [S, n_bus]; v_init: complex128 [S, n_bus] or None (flat start); u_pu: float64
         [n_bus] flat-start |V| of SLACK/PV buses.  refine_below > 0 runs the `refine`
         refinement steps only in iterations where a scenario of the lane group has max
-        |mismatch| below it."""
+        |mismatch| below it.  reuse_below > 0 keeps a group's previous LU factors once all
+        its iterating scenarios are below it (the refined solve then corrects against the
+        current Jacobian; needs refine >= 1)."""
         torch = _torch()
         n = self.plan.info["n_bus"]
         dev = s_spec.device
@@ -253,7 +257,8 @@ class NRBatch:
                            torch.empty(self.n_scen, dtype=torch.int32, device=dev),
                            torch.empty(self.n_scen, dtype=torch.int32, device=dev),
                            torch.empty(self.n_scen, dtype=torch.float64, device=dev))
-        inp = self._inputs(y, s_spec, v_init, u_pu, tol, max_iter, policy, refine, refine_below)
+        inp = self._inputs(y, s_spec, v_init, u_pu, tol, max_iter, policy, refine, refine_below,
+                           reuse_below)
         o = N.Outputs(_dptr(out.v), _dptr(out.iterations), _dptr(out.status),
                       _dptr(out.final_mismatch))
         N.check(N.lib().gapk_nr_solve(self._h, C.byref(inp), C.byref(o), _stream_ptr(stream)))

@@ -148,7 +148,7 @@ _TUNED: "weakref.WeakKeyDictionary[NRPlan, dict]" = weakref.WeakKeyDictionary()
 
 
 def autotune(study: Study, tol=1e-8, max_iter=20, policy="newton", refine=1,
-             candidates=CANDIDATES, reps=2, refine_below=0.0):
+             candidates=CANDIDATES, reps=2, refine_below=0.0, reuse_below=0.0):
     """Time each (lanes, threads) candidate on the study's own inputs (CUDA events, after a
     warm-up solve) and keep the fastest batch in the study.  Candidates whose lane count
     exceeds the scenario count are skipped; results are cached per (plan, S, precision,
@@ -169,14 +169,16 @@ def autotune(study: Study, tol=1e-8, max_iter=20, policy="newton", refine=1,
         b = NRBatch(study.plan, study.n_scen, precision=study.precision,
                     y_shared=study.y_shared, lanes=lanes, threads=threads)
         b.solve(study.y, study.s_spec, v_init=study.v0, tol=tol, max_iter=max_iter,
-                policy=policy, refine=refine, refine_below=refine_below)
+                policy=policy, refine=refine, refine_below=refine_below,
+                reuse_below=reuse_below)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(reps):
             b.solve(study.y, study.s_spec, v_init=study.v0, tol=tol, max_iter=max_iter,
-                    policy=policy, refine=refine, refine_below=refine_below)
+                    policy=policy, refine=refine, refine_below=refine_below,
+                reuse_below=reuse_below)
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
@@ -192,7 +194,7 @@ def autotune(study: Study, tol=1e-8, max_iter=20, policy="newton", refine=1,
 
 
 def solve_concurrent(studies, tol=1e-8, max_iter=20, policy="newton", refine=1,
-                     refine_below=0.0):
+                     refine_below=0.0, reuse_below=0.0):
     """Launch every study on its own CUDA stream (inputs made visible to it first) and wait
     for all of them.  Each study's result lands in `study.result`."""
     torch = _torch()
@@ -206,7 +208,8 @@ def solve_concurrent(studies, tol=1e-8, max_iter=20, policy="newton", refine=1,
         with torch.cuda.stream(st.stream):
             st.result = st.batch.solve(st.y, st.s_spec, v_init=st.v0, tol=tol,
                                        max_iter=max_iter, policy=policy, refine=refine,
-                                       stream=st.stream, refine_below=refine_below)
+                                       stream=st.stream, refine_below=refine_below,
+                                       reuse_below=reuse_below)
     for st in studies:
         cur.wait_stream(st.stream)
     return [st.result for st in studies]

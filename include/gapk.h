@@ -209,6 +209,10 @@ typedef struct {
     double refine_below;    /* refine only in iterations where some iterating scenario of a
                                lane group has max |mismatch| below this (0 = every iteration);
                                far from the solution the FP32 step error does not slow Newton */
+    double reuse_below;     /* once every iterating scenario of a lane group has max |mismatch|
+                               below this, the group keeps its previous LU factors instead of
+                               refactorising, and the (refined, refine >= 1) solve uses them
+                               against the current FP64 Jacobian (0 = refactorise every time) */
 } gapk_nr_inputs;
 
 typedef struct {

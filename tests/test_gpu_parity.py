@@ -457,3 +457,42 @@ def test_host_pipeline_equals_one_batch():
         assert torch.equal(vo, one.v.cpu())
         assert torch.equal(st, one.status.cpu()) and (st.numpy() == 0).all()
         assert torch.equal(it, one.iterations.cpu())
+
+
+def test_factor_reuse_near_convergence_matches_oracle():
+    """Below reuse_below a lane group keeps its previous LU factors and the refined solve
+    corrects against the current FP64 Jacobian: converged voltages as the FP64 oracle's, and
+    the option is refused without refinement."""
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.transmission_grid(1, n=2000)
+    base = 1e8
+    zb = net.u_rated[0] ** 2 / base
+    S = 13
+    s_spec = synth.load_scenarios(net, S, sigma=0.1, seed=7, base_power=base)
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
+    v0 = np.repeat(synth.dc_start(net, base)[None], S, axis=0)
+    s_t = torch.as_tensor(s_spec, device="cuda")
+    v_t = torch.as_tensor(v0, device="cuda")
+    Y = restate.ybus_pi(net)
+    for lanes, n_sc in ((4, S), (8, 320)):
+        b = NRBatch(plan, n_sc, precision="fp32", lanes=lanes)
+        ss = s_t if n_sc == S else s_t.repeat((n_sc + S - 1) // S, 1)[:n_sc].contiguous()
+        vv = v_t if n_sc == S else v_t.repeat((n_sc + S - 1) // S, 1)[:n_sc].contiguous()
+        r = b.solve(y, ss, v_init=vv, tol=1e-10, max_iter=30, policy="newton", refine=1,
+                    refine_below=1e-3, reuse_below=1e-3)
+        torch.cuda.synchronize()
+        assert (r.status.cpu().numpy() == 0).all()
+        V = r.v.cpu().numpy()
+        for s in (0, 6, 12):
+            o = restate.nr_solve(net, Y=Y, tol=1e-12, max_iter=30, base_power=base,
+                                 policy="newton", jac="exact", s_spec=s_spec[s], v0=v0[s])
+            assert np.max(np.abs(V[s] - o["v"])) < 1e-8
+    with pytest.raises(Exception):
+        b.solve(y, ss, v_init=vv, tol=1e-10, max_iter=30, policy="newton", refine=0,
+                reuse_below=1e-3)
