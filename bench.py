@@ -10,6 +10,7 @@ every rank solves its own 1024 scenarios of the same grid.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --workload mixed     # the mixed batch below, one JSON line
     python bench.py --workload large     # the 100k-bus grid below, one JSON line
+    python bench.py --workload adjoint   # loss gradients on 256 scenarios, one JSON line
 
 Prints one JSON line (rank 0).  `value` times the solve with inputs resident in HBM; `e2e`
 times the same call with host (pinned) inputs and results copied inside the timed region.
@@ -597,6 +598,61 @@ def run_large(args):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args):
+    import numpy as np
+    import torch
+
+    from gap_b200 import synth
+    from gap_b200.autograd import DifferentiablePowerFlow, branch_losses_mw
+
+    net = synth.transmission_grid(GRID_SEED, n=N_BUS)
+    S = 256
+    s = synth.load_scenarios(net, S, sigma=SIGMA, seed=1, base_power=BASE)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        model = DifferentiablePowerFlow(net, S, base_power=BASE, precision=prec, tol=1e-10,
+                                        max_iter=30)
+        p = torch.tensor(s.real, device="cuda", requires_grad=True)
+        q = torch.tensor(s.imag, device="cuda", requires_grad=True)
+        r = model.branch[:, 0].clone().requires_grad_(True)
+        x = model.branch[:, 1].clone().requires_grad_(True)
+
+        def step():
+            for t in (p, q, r, x):
+                t.grad = None
+            vm, va = model(p, q, r, x)
+            L = ((vm - 1.0) ** 2).sum() + branch_losses_mw(vm, va, r, x, model).sum()
+            L.backward()
+            return L
+
+        for _ in range(max(args.warmup, 1)):
+            step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            L = step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        out[prec] = {"ms_per_step": ms, "gradients_per_s": S / (ms / 1e3),
+                     "loss": float(L.item()),
+                     "grad_norms": [float(t.grad.norm().item()) for t in (p, q, r, x)]}
+    line = {
+        "metric": "Loss gradients/s on 1 B200 (power flow + adjoint, dL/dP, dL/dQ per bus and "
+                  "dL/dr, dL/dx per branch)",
+        "workload": "adjoint", "value": out["fp64"]["gradients_per_s"], "unit": "gradients/s",
+        "n_gpus": 1, "steps": args.steps, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded generator, no external dataset)",
+        "config": {"workload": f"{S} load scenarios x {N_BUS}-bus transmission grid "
+                               f"(seed {GRID_SEED})",
+                   "loss": "sum_bus (|V|-1)^2 + sum_branch P_loss [MW]", "tol_pu": 1e-10},
+        "fp64": out["fp64"], "fp32_factor_refined": out["fp32"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_SCEN
     ap = argparse.ArgumentParser()
@@ -608,7 +664,7 @@ def main():
                     help="scenarios per GPU (profiling runs use fewer; the headline uses 1024)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling)")
     ap.add_argument("--workload", default="transmission",
-                    choices=["transmission", "mixed", "large"],
+                    choices=["transmission", "mixed", "large", "adjoint"],
                     help="transmission: the headline; mixed / large: supplementary lines")
     ap.add_argument("--large-buses", type=int, default=100_000,
                     help="grid size of --workload large")
@@ -627,7 +683,7 @@ def main():
 
     torch.cuda.set_device(local)
     if args.workload != "transmission":
-        (run_mixed if args.workload == "mixed" else run_large)(args)
+        {"mixed": run_mixed, "large": run_large, "adjoint": run_adjoint}[args.workload](args)
         return
     if world > 1:
         import datetime

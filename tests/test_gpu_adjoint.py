@@ -115,3 +115,24 @@ def test_fp32_factors_with_refinement_match_fp64_gradients():
         outs.append([t.grad.cpu().numpy() for t in (p, q, r, x)])
     for a, b in zip(*outs):
         assert _rel_ok(b, a) < REL
+
+
+def test_adjoint_at_transmission_scale():
+    """The C4 setting on fewer scenarios: 10k-bus grid, gradients of the same loss against
+    the FP64 oracle's implicit-function gradient (1e-6 relative)."""
+    import torch
+
+    net, s, model, p, q, r, x = _setup(n=10_000, S=2, seed=0, tol=1e-10)
+    L, vm, va = _loss(model, p, q, r, x)
+    L.backward()
+    v = (vm.detach() * torch.exp(1j * va.detach())).cpu().numpy()
+    dr_tot = np.zeros(net.n_branch)
+    dx_tot = np.zeros(net.n_branch)
+    for k in range(s.shape[0]):
+        o = restate.adjoint_gradients(net, v[k], base_power=model.base_power, taps=True)
+        assert _rel_ok(p.grad[k].cpu().numpy(), o["dP"]) < REL
+        assert _rel_ok(q.grad[k].cpu().numpy(), o["dQ"]) < REL
+        dr_tot += o["dr"]
+        dx_tot += o["dx"]
+    assert _rel_ok(r.grad.cpu().numpy(), dr_tot) < REL
+    assert _rel_ok(x.grad.cpu().numpy(), dx_tot) < REL
