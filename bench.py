@@ -11,6 +11,7 @@ every rank solves its own 1024 scenarios of the same grid.
     python bench.py --workload mixed     # the mixed batch below, one JSON line
     python bench.py --workload large     # the 100k-bus grid below, one JSON line
     python bench.py --workload adjoint   # loss gradients on 256 scenarios, one JSON line
+    python bench.py --workload feeder    # the 200-bus feeder, with the reference's CPU time
 
 Prints one JSON line (rank 0).  `value` times the solve with inputs resident in HBM; `e2e`
 times the same call with host (pinned) inputs and results copied inside the timed region.
@@ -653,6 +654,79 @@ def run_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+def run_feeder(args):
+    """the 200-bus meshed feeder, where the reference's own CPU backend is timeable.
+    Reference step policy (the reference's damped, clamped update), tol 1e-8 pu, flat start."""
+    import numpy as np
+    import torch
+
+    from gap_b200 import _native as N
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    base = 1e6
+    net = synth.feeder_grid(0)
+    zb = float(net.u_rated[0]) ** 2 / base
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=N.YBUS_REFERENCE,
+                    scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type)
+    u = torch.as_tensor(net.u_pu.astype(np.float64), device="cuda")
+    kw = dict(tol=1e-8, max_iter=20, policy="reference", u_pu=u)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    res = {}
+    for name, S in (("single_fp64", 1), ("batched_fp64", 1024)):
+        s = (net.specified_power(base)[None] if S == 1 else
+             synth.load_scenarios(net, S, sigma=SIGMA, seed=1, base_power=base))
+        st = torch.as_tensor(s, device="cuda")
+        b = NRBatch(plan, S, precision="fp64", lanes=1 if S == 1 else 8,
+                    threads=256 if S == 1 else 512)
+        for _ in range(max(args.warmup, 1)):
+            r = b.solve(y, st, **kw)
+        torch.cuda.synchronize()
+        reps = max(args.steps, 5)
+        e0.record()
+        for _ in range(reps):
+            r = b.solve(y, st, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        conv = int((r.status == 0).sum().item())
+        res[name] = {"solves_per_s": conv / (ms / 1e3), "ms_per_batch": ms, "scenarios": S,
+                     "converged": conv, "iterations_max": int(r.iterations.max().item())}
+    cpu = None
+    try:
+        from oracle import refnet  # the reference's own CPU backend, built from its sources
+
+        if refnet.available():
+            refnet.solve(net, tol=1e-8, max_iter=20, base_power=base)  # warm-up
+            t0 = time.perf_counter()
+            o = refnet.solve(net, tol=1e-8, max_iter=20, base_power=base)
+            wall = time.perf_counter() - t0
+            cpu = {"value": 1.0 / wall if o["converged"] else 0.0, "unit": "solves/s",
+                   "cores": 1, "kind": "reference",
+                   "sample": f"one solve of the same feeder by the reference's CPU backend "
+                             f"(dense Jacobian, its LU), {o['iterations']} iterations, "
+                             f"{wall:.2f} s"}
+    except Exception as e:  # the compiled reference is optional on a box without it
+        cpu = {"unavailable": str(e)[:200]}
+    line = {
+        "metric": "Power-flow solves/s on 1 B200, 200-bus meshed feeder (reference step "
+                  "policy, FP64) at 1e-8 pu",
+        "workload": "feeder", "value": res["batched_fp64"]["solves_per_s"], "unit": "solves/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded generator, no external dataset)",
+        "config": {"workload": "200-bus meshed feeder (seed 0); 1024 lognormal load scenarios "
+                               "for the batched line", "policy": "reference", "tol_pu": 1e-8,
+                   "start": "flat"},
+        "single_fp64": res["single_fp64"], "batched_fp64": res["batched_fp64"],
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_SCEN
     ap = argparse.ArgumentParser()
@@ -664,7 +738,7 @@ def main():
                     help="scenarios per GPU (profiling runs use fewer; the headline uses 1024)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling)")
     ap.add_argument("--workload", default="transmission",
-                    choices=["transmission", "mixed", "large", "adjoint"],
+                    choices=["transmission", "mixed", "large", "adjoint", "feeder"],
                     help="transmission: the headline; mixed / large: supplementary lines")
     ap.add_argument("--large-buses", type=int, default=100_000,
                     help="grid size of --workload large")
@@ -683,7 +757,8 @@ def main():
 
     torch.cuda.set_device(local)
     if args.workload != "transmission":
-        {"mixed": run_mixed, "large": run_large, "adjoint": run_adjoint}[args.workload](args)
+        {"mixed": run_mixed, "large": run_large, "adjoint": run_adjoint,
+         "feeder": run_feeder}[args.workload](args)
         return
     if world > 1:
         import datetime
