@@ -283,8 +283,9 @@ __global__ void k_check(BatchDev B, int use_cond, cudaGraphConditionalHandle han
 __device__ __forceinline__ void polar_parts(double2 v, double& vmr, double& c, double& s) {
     const double vm = hypot(v.x, v.y);
     if (vm > 0.0) {
-        c = v.x / vm;
-        s = v.y / vm;
+        const double inv = 1.0 / vm;  // one division for both direction cosines
+        c = v.x * inv;
+        s = v.y * inv;
     } else {
         c = 1.0;
         s = 0.0;
@@ -320,9 +321,10 @@ __global__ void __launch_bounds__(256) k_jfill(PlanDev P, BatchDev B) {
         if (diag) {
             const double2 S = B.Scalc[((size_t)g * n + si.x) * SW + lane];
             J.a = -S.y - Bv * vmi * vmi;
-            J.b = S.x / vmi + G * vmi;
+            const double ivm = 1.0 / vmi;
+            J.b = S.x * ivm + G * vmi;
             J.c = S.x - G * vmi * vmi;
-            J.d = S.y / vmi - Bv * vmi;
+            J.d = S.y * ivm - Bv * vmi;
             if (!pqi) {
                 J.b = 0.0;
                 J.c = 0.0;
