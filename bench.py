@@ -655,7 +655,7 @@ def run_adjoint(args):
 
 
 def run_feeder(args):
-    """the 200-bus meshed feeder, where the reference's own CPU backend is timeable.
+    """The 200-bus meshed feeder, the one size where the reference's own CPU backend finishes.
     Reference step policy (the reference's damped, clamped update), tol 1e-8 pu, flat start."""
     import numpy as np
     import torch
