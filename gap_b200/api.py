@@ -6,6 +6,9 @@ Mirrors the reference's interfaces for the Newton-Raphson path:
 * `AdmittanceMatrix.build_admittance_matrix`  include/gap/admittance/admittance_interface.h:21
 * `NewtonRaphson.solve_power_flow` / `.calculate_mismatches`
                                               include/gap/solver/powerflow_interface.h:59-79
+* `IterationState`, `NewtonRaphson.enable_state_capture` / `.get_iteration_states` /
+  `.clear_iteration_states`                   include/gap/solver/powerflow_interface.h:28-35,
+                                              83-107
 * `solve_simple_power_flow`                   bindings/solver_bindings.cpp:56-217 (same
                                               argument lists, same output rows)
 
@@ -55,6 +58,19 @@ class PowerFlowResult:
     status: int = N.SCEN_MAXITER
 
 
+@dataclass
+class IterationState:
+    """gap::solver::IterationState (powerflow_interface.h:28-35): the state one iteration's
+    mismatch is taken at, per unit; mismatches in the reference's equation order."""
+
+    iteration: int
+    voltages: np.ndarray
+    currents: np.ndarray
+    power_injections: np.ndarray
+    mismatches: np.ndarray
+    max_mismatch: float
+
+
 class AdmittanceMatrix:
     """GPU Y-bus builder (IAdmittanceMatrix).  Returns the CSR triple in Siemens."""
 
@@ -98,6 +114,8 @@ class NewtonRaphson:
     def __init__(self):
         self._plans = {}
         self._batches = {}
+        self._capture = False
+        self._states = []
 
     def _plan(self, row_ptr, col_idx, bus_type, jac):
         key = (np.asarray(row_ptr, np.int32).tobytes(), np.asarray(col_idx, np.int32).tobytes(),
@@ -144,9 +162,28 @@ class NewtonRaphson:
         batch = self._batch(plan, config.precision)
         s = torch.as_tensor(net.specified_power(config.base_power)[None, :], device="cuda")
         u = torch.as_tensor(net.u_pu, dtype=torch.float64, device="cuda")
-        r = batch.solve(y, s, u_pu=u, tol=config.tolerance, max_iter=config.max_iterations,
-                        policy=config.policy, refine=config.refine)
-        torch.cuda.synchronize()
+        kw = dict(u_pu=u, tol=config.tolerance, max_iter=config.max_iterations,
+                  policy=config.policy, refine=config.refine)
+        if self._capture:
+            r, states = batch.solve_captured(y, s, **kw)
+            torch.cuda.synchronize()
+            self._states = [IterationState(
+                iteration=int(x["iteration"]), voltages=x["v"][0].cpu().numpy(),
+                currents=x["i"][0].cpu().numpy(), power_injections=x["s"][0].cpu().numpy(),
+                mismatches=x["mismatch"][0].cpu().numpy(),
+                max_mismatch=float(x["max_mismatch"][0].item())) for x in states]
+            if int(r.status[0].item()) == N.SCEN_SINGULAR:
+                # the device loop stops a scenario whose Jacobian does not factorise; the
+                # reference keeps V and runs on to max_iterations (cpu_newton_raphson.cpp:
+                # 416-419), recording the same state each time
+                while self._states and len(self._states) < int(r.iterations[0].item()):
+                    last = self._states[-1]
+                    self._states.append(IterationState(len(self._states), last.voltages,
+                                                       last.currents, last.power_injections,
+                                                       last.mismatches, last.max_mismatch))
+        else:
+            r = batch.solve(y, s, **kw)
+            torch.cuda.synchronize()
         st = int(r.status[0].item())
         return PowerFlowResult(converged=st == N.SCEN_CONVERGED,
                                iterations=int(r.iterations[0].item()),
@@ -176,6 +213,18 @@ class NewtonRaphson:
         f = batch.mismatch()
         torch.cuda.synchronize()
         return f[0].cpu().numpy() * base
+
+    def enable_state_capture(self, enable: bool):
+        """Record an IterationState per iteration of each following solve (the device loop is
+        then stepped from the host, one synchronisation per iteration; same trajectory).  The
+        states of the last solve replace the previous ones, as gpu_newton_raphson.cu:402-405."""
+        self._capture = bool(enable)
+
+    def get_iteration_states(self):
+        return self._states
+
+    def clear_iteration_states(self):
+        self._states = []
 
     def set_lu_solver(self, lu_solver):
         """Accepted for interface compatibility: the device-resident engine factorises the

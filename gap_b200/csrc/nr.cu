@@ -397,6 +397,15 @@ struct ToRefOp {
     }
 };
 
+template <typename T, int SW>
+struct StateOp {
+    static void run(gapk_nr_batch b, double2* v, double2* i, double2* s, cudaStream_t st) {
+        long total = (long)b->n_scen * b->plan->dev.n_bus;
+        if (total == 0) return;
+        k_state<SW><<<blocks_for(total, 256), 256, 0, st>>>(b->plan->dev, b->dev, v, i, s);
+    }
+};
+
 int check_launch() {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -859,6 +868,41 @@ int gapk_nr_stage_get_mismatch(gapk_nr_batch b, double* d_f, void* stream) {
     if (!b || !d_f) return GAPK_EINVAL;
     dispatch_tsw<ToRefOp>(b->precision, b->sw, b, b->dev.rhs, b->plan->d_eq.as<int>(),
                           b->plan->h.n_vars, -1.0, d_f, static_cast<cudaStream_t>(stream));
+    return check_launch();
+}
+
+int gapk_nr_step(gapk_nr_batch b, int* h_active, void* stream) {
+    if (!b || !h_active) {
+        set_error("gapk_nr_step: bad arguments");
+        return GAPK_EINVAL;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    dispatch_tsw<BodyOp>(b->precision, b->sw, b, st, 0, cudaGraphConditionalHandle{});
+    int rc = check_launch();
+    if (rc) return rc;
+    GAPK_CUDA_TRY(cudaMemcpyAsync(h_active, b->dev.ctrl + 2, sizeof(int),
+                                  cudaMemcpyDeviceToHost, st));
+    GAPK_CUDA_TRY(cudaStreamSynchronize(st));
+    return GAPK_OK;
+}
+
+int gapk_nr_get_state(gapk_nr_batch b, double* d_v, double* d_i, double* d_s, void* stream) {
+    if (!b) {
+        set_error("gapk_nr_get_state: null batch");
+        return GAPK_EINVAL;
+    }
+    dispatch_tsw<StateOp>(b->precision, b->sw, b, reinterpret_cast<double2*>(d_v),
+                          reinterpret_cast<double2*>(d_i), reinterpret_cast<double2*>(d_s),
+                          static_cast<cudaStream_t>(stream));
+    return check_launch();
+}
+
+int gapk_nr_get_outputs(gapk_nr_batch b, const gapk_nr_outputs* out, void* stream) {
+    if (!b || !out) {
+        set_error("gapk_nr_get_outputs: bad arguments");
+        return GAPK_EINVAL;
+    }
+    dispatch_tsw<StoreOp>(b->precision, b->sw, b, out, static_cast<cudaStream_t>(stream));
     return check_launch();
 }
 

@@ -1228,6 +1228,35 @@ __global__ void k_store(PlanDev P, BatchDev B, double2* v_out, int* it_out, int*
     }
 }
 
+// current state per scenario in bus order: V, I = Y V and S = V conj(I), per unit
+// (IterationState of powerflow_interface.h:28-35, filled as cpu_newton_raphson.cpp:125-149)
+template <int SW>
+__global__ void k_state(PlanDev P, BatchDev B, double2* v_out, double2* i_out,
+                        double2* s_out) {
+    const int n = P.n_bus;
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long)B.n_scen * n) return;
+    const int s = (int)(tid / n), i = (int)(tid % n);
+    const int g = s / SW, lane = s % SW;
+    const double2* Vg = B.V + (size_t)g * n * SW;
+    const double2* Yg = B.y_shared ? B.Y : B.Y + (size_t)g * P.nnz_y * SW;
+    const size_t ys = B.y_shared ? 1 : SW;
+    const size_t yl = B.y_shared ? 0 : lane;
+    double ir = 0.0, ii = 0.0;
+    for (int p = P.y_row_ptr[i]; p < P.y_row_ptr[i + 1]; ++p) {
+        const double2 y = Yg[(size_t)p * ys + yl];
+        const double2 v = Vg[(size_t)P.y_col[p] * SW + lane];
+        ir = fma(y.x, v.x, ir);
+        ir = fma(-y.y, v.y, ir);
+        ii = fma(y.x, v.y, ii);
+        ii = fma(y.y, v.x, ii);
+    }
+    const double2 vi = Vg[(size_t)i * SW + lane];
+    if (v_out) v_out[tid] = vi;
+    if (i_out) i_out[tid] = make_double2(ir, ii);
+    if (s_out) s_out[tid] = make_double2(fma(vi.x, ir, vi.y * ii), fma(vi.y, ir, -vi.x * ii));
+}
+
 // node vector [G][nb][SW] -> reference order [n_scen][n_vars]; map[node*2+c] gives the
 // reference index (or -1); sign multiplies the value
 template <int SW>

@@ -8,7 +8,8 @@
 // loop runs on the device; the plan (ordering, symbolic factorisation) is cached per Y pattern
 // and bus-type vector and rebuilt when either changes.  config.acceleration_factor is ignored,
 // as by the reference CPU solver.  set_lu_solver() is accepted but the device engine always
-// factorises with its own block LU.
+// factorises with its own block LU.  With state capture enabled the same device loop is stepped
+// from the host, one synchronisation per iteration.
 #include <cmath>
 #include <unordered_map>
 
@@ -58,7 +59,10 @@ class B200NewtonRaphson final : public gap::solver::IPowerFlowSolver {
         out.d_iterations = static_cast<int*>(d_it_.ensure(4));
         out.d_status = static_cast<int*>(d_st_.ensure(4));
         out.d_final_mismatch = static_cast<double*>(d_fm_.ensure(8));
-        check(gapk_nr_solve(batch_, &in, &out, nullptr), "gapk_nr_solve");
+        if (capture_)
+            solve_capturing(in, out, n, cfg.max_iterations);
+        else
+            check(gapk_nr_solve(batch_, &in, &out, nullptr), "gapk_nr_solve");
         check_cuda(cudaMemcpy(res.bus_voltages.data(), out.d_v, static_cast<size_t>(n) * 16,
                               cudaMemcpyDeviceToHost),
                    "cudaMemcpy D2H");
@@ -67,6 +71,16 @@ class B200NewtonRaphson final : public gap::solver::IPowerFlowSolver {
         check_cuda(cudaMemcpy(&it, out.d_iterations, 4, cudaMemcpyDeviceToHost), "D2H");
         check_cuda(cudaMemcpy(&st, out.d_status, 4, cudaMemcpyDeviceToHost), "D2H");
         check_cuda(cudaMemcpy(&fm, out.d_final_mismatch, 8, cudaMemcpyDeviceToHost), "D2H");
+        if (capture_ && st == GAPK_SCEN_SINGULAR) {
+            // the device loop stops a scenario whose Jacobian does not factorise; the reference
+            // keeps V and runs on to max_iterations (cpu_newton_raphson.cpp:416-419), recording
+            // the same state each time
+            while (!states_.empty() && static_cast<int>(states_.size()) < it) {
+                gap::solver::IterationState s = states_.back();
+                s.iteration = static_cast<int>(states_.size());
+                states_.push_back(std::move(s));
+            }
+        }
         res.converged = st == GAPK_SCEN_CONVERGED;
         res.iterations = it;
         res.final_mismatch = fm;
@@ -108,7 +122,49 @@ class B200NewtonRaphson final : public gap::solver::IPowerFlowSolver {
         return gap::BackendType::GPU_CUDA;
     }
 
+    // Iteration-state capture (powerflow_interface.h:83-107): with capture enabled, each solve
+    // records, per iteration, the voltages the mismatch is taken at, I = Y V, S = V conj(I),
+    // the mismatches (per unit, in the reference's equation order) and their maximum, as
+    // gpu_newton_raphson.cu:452-490 and cpu_newton_raphson.cpp:125-149 do.
+    void enable_state_capture(bool enable) override { capture_ = enable; }
+    std::vector<gap::solver::IterationState> const& get_iteration_states() const override {
+        return states_;
+    }
+    void clear_iteration_states() override { states_.clear(); }
+
   private:
+    // The device loop stepped one iteration at a time (the trajectory of gapk_nr_solve) with
+    // the state copied out before each step and the step's mismatch after it.
+    void solve_capturing(gapk_nr_inputs const& in, gapk_nr_outputs const& out, int n,
+                         int max_iterations) {
+        states_.clear();
+        check(gapk_nr_stage_load(batch_, &in, nullptr), "gapk_nr_stage_load");
+        gapk_nr_plan_info info{};
+        check(gapk_nr_plan_get_info(plan_, &info), "gapk_nr_plan_get_info");
+        double* dv = static_cast<double*>(d_cap_.ensure(static_cast<size_t>(n) * 48));
+        double* df = static_cast<double*>(d_f_.ensure(static_cast<size_t>(info.n_vars) * 8 + 8));
+        std::vector<gap::Complex> vis;
+        for (int it = 0; it < max_iterations; ++it) {
+            check(gapk_nr_get_state(batch_, dv, dv + 2 * n, dv + 4 * n, nullptr),
+                  "gapk_nr_get_state");
+            int active = 0;
+            check(gapk_nr_step(batch_, &active, nullptr), "gapk_nr_step");
+            check(gapk_nr_stage_get_mismatch(batch_, df, nullptr), "gapk_nr_stage_get_mismatch");
+            gap::solver::IterationState s;
+            s.iteration = it;
+            d_cap_.download(vis, static_cast<size_t>(3) * n);
+            s.voltages.assign(vis.begin(), vis.begin() + n);
+            s.currents.assign(vis.begin() + n, vis.begin() + 2 * n);
+            s.power_injections.assign(vis.begin() + 2 * n, vis.end());
+            d_f_.download(s.mismatches, info.n_vars);
+            s.max_mismatch = 0.0;
+            for (double x : s.mismatches) s.max_mismatch = std::max(s.max_mismatch, std::abs(x));
+            states_.push_back(std::move(s));
+            if (!active) break;
+        }
+        check(gapk_nr_get_outputs(batch_, &out, nullptr), "gapk_nr_get_outputs");
+    }
+
     // get_specified_power_at_bus (cpu_newton_raphson.cpp:346-377), per unit of `base`
     static std::vector<gap::Complex> specified_power(gap::NetworkData const& net, double base) {
         const int n = static_cast<int>(net.buses.size());
@@ -159,7 +215,9 @@ class B200NewtonRaphson final : public gap::solver::IPowerFlowSolver {
     gapk_nr_plan plan_ = nullptr;
     gapk_nr_batch batch_ = nullptr;
     std::vector<int> bt_, rp_, ci_;
-    DeviceBuffer d_y_, d_s_, d_u_, d_v_, d_vo_, d_it_, d_st_, d_fm_, d_f_;
+    bool capture_ = false;
+    std::vector<gap::solver::IterationState> states_;
+    DeviceBuffer d_y_, d_s_, d_u_, d_v_, d_vo_, d_it_, d_st_, d_fm_, d_f_, d_cap_;
 };
 
 }  // namespace gapb200

@@ -264,6 +264,45 @@ class NRBatch:
         N.check(N.lib().gapk_nr_solve(self._h, C.byref(inp), C.byref(o), _stream_ptr(stream)))
         return out
 
+    def solve_captured(self, y, s_spec, v_init=None, u_pu=None, tol=1e-8, max_iter=20,
+                       policy="reference", refine=0, stream=None, refine_below=0.0,
+                       reuse_below=0.0):
+        """solve() stepped one iteration at a time, recording per iteration what
+        IPowerFlowSolver's state capture records (powerflow_interface.h:28-35,
+        gpu_newton_raphson.cu:452-490): the voltages that iteration's mismatch is taken at,
+        I = Y V, S = V conj(I) (complex128 [S, n_bus], per unit), the mismatch in the
+        reference's equation order ([S, n_vars]) and its max |.| per scenario.  The trajectory
+        is solve()'s.  Returns (NRResult, list of dicts with keys iteration, v, i, s,
+        mismatch, max_mismatch)."""
+        torch = _torch()
+        n = self.plan.info["n_bus"]
+        dev = s_spec.device
+        sp = _stream_ptr(stream)
+        inp = self._inputs(y, s_spec, v_init, u_pu, tol, max_iter, policy, refine, refine_below,
+                           reuse_below)
+        N.check(N.lib().gapk_nr_stage_load(self._h, C.byref(inp), sp))
+        states = []
+        active = C.c_int(0)
+        for it in range(int(max_iter)):
+            v, i, s = (torch.empty((self.n_scen, n), dtype=torch.complex128, device=dev)
+                       for _ in range(3))
+            N.check(N.lib().gapk_nr_get_state(self._h, _dptr(v), _dptr(i), _dptr(s), sp))
+            N.check(N.lib().gapk_nr_step(self._h, C.byref(active), sp))
+            f = self.mismatch(stream)
+            states.append(dict(iteration=it, v=v, i=i, s=s, mismatch=f,
+                               max_mismatch=f.abs().amax(dim=1) if f.shape[1] else
+                               torch.zeros(self.n_scen, dtype=torch.float64, device=dev)))
+            if not active.value:
+                break
+        out = NRResult(torch.empty((self.n_scen, n), dtype=torch.complex128, device=dev),
+                       torch.empty(self.n_scen, dtype=torch.int32, device=dev),
+                       torch.empty(self.n_scen, dtype=torch.int32, device=dev),
+                       torch.empty(self.n_scen, dtype=torch.float64, device=dev))
+        o = N.Outputs(_dptr(out.v), _dptr(out.iterations), _dptr(out.status),
+                      _dptr(out.final_mismatch))
+        N.check(N.lib().gapk_nr_get_outputs(self._h, C.byref(o), sp))
+        return out, states
+
     # stage access (tests, profiling)
     def stage_load(self, y, s_spec, v_init=None, u_pu=None, refine=0, stream=None,
                    policy="newton"):

@@ -226,6 +226,22 @@ typedef struct {
 int gapk_nr_solve(gapk_nr_batch b, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
                   void* stream);
 
+/* ==== Stepping, for iteration-state capture ===============================================
+ * IPowerFlowSolver::enable_state_capture / get_iteration_states
+ * (include/gap/solver/powerflow_interface.h:28-35,83-107; recorded per iteration by
+ * src/solver/powerflow/gpu/gpu_newton_raphson.cu:452-490).  After gapk_nr_stage_load, each
+ * gapk_nr_step runs one iteration of the loop gapk_nr_solve runs (mismatch, convergence test,
+ * Jacobian, factorisation, solve, update) on every scenario still iterating, synchronises the
+ * stream and sets *h_active to 1 while some scenario is still iterating.  At most
+ * max_iterations steps do work; gapk_nr_get_outputs then writes what gapk_nr_solve writes.
+ * The trajectory is the one gapk_nr_solve takes. */
+int gapk_nr_step(gapk_nr_batch b, int* h_active, void* stream);
+/* The batch's current state in bus order, per unit, complex [n_scen][n_bus] each (any may be
+ * NULL): the voltages V, the current injections I = Y V and the power injections
+ * S = V conj(I).  Called before a step, it is the state that step's mismatch is taken at. */
+int gapk_nr_get_state(gapk_nr_batch b, double* d_v, double* d_i, double* d_s, void* stream);
+int gapk_nr_get_outputs(gapk_nr_batch b, const gapk_nr_outputs* out, void* stream);
+
 /* ==== Adjoint (gradients through the converged state; no counterpart in the reference) ====
  * With the batch holding a converged state (after gapk_nr_solve, or gapk_nr_stage_load with
  * the solution as d_v_init), refactorises the Jacobian at that state and solves

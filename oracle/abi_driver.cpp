@@ -146,6 +146,49 @@ int main(int argc, char** argv) {
     std::cout << "mismatch_sizes " << mc.size() << " " << mg.size() << "\nmismatch_max_abs_diff "
               << dm << " " << sm << "\n";
 
+    // iteration-state capture: per-iteration states of both solvers along their trajectories
+    // (differences relative to each quantity's largest magnitude over the run), and the
+    // capturing solve's result against the plain one
+    solver::IPowerFlowSolver& cbase = cnr;  // the capture methods are public on the interface
+    cbase.enable_state_capture(true);
+    gnr->enable_state_capture(true);
+    cnr.solve_power_flow(net, *Yc, cfg);
+    auto rg2 = gnr->solve_power_flow(net, *Yg, cfg);
+    auto const& sc = cbase.get_iteration_states();
+    auto const& sg = gnr->get_iteration_states();
+    auto rel = [](std::vector<Complex> const& a, std::vector<Complex> const& b) {
+        double d = 0.0, s = 0.0;
+        for (size_t i = 0; i < a.size() && i < b.size(); ++i) {
+            d = std::max(d, std::abs(a[i] - b[i]));
+            s = std::max(s, std::abs(a[i]));
+        }
+        return a.size() == b.size() ? (s > 0 ? d / s : d) : 1e300;
+    };
+    double cv = 0.0, ci = 0.0, cs = 0.0, cm = 0.0, cx = 0.0, m0 = 0.0;
+    int idx_ok = 1;
+    for (auto const& st : sc) m0 = std::max(m0, st.max_mismatch);
+    for (size_t k = 0; k < sc.size() && k < sg.size(); ++k) {
+        idx_ok &= sc[k].iteration == static_cast<int>(k) && sg[k].iteration == static_cast<int>(k);
+        cv = std::max(cv, rel(sc[k].voltages, sg[k].voltages));
+        ci = std::max(ci, rel(sc[k].currents, sg[k].currents));
+        cs = std::max(cs, rel(sc[k].power_injections, sg[k].power_injections));
+        if (sc[k].mismatches.size() != sg[k].mismatches.size()) cm = 1e300;
+        for (size_t i = 0; i < sc[k].mismatches.size() && i < sg[k].mismatches.size(); ++i)
+            cm = std::max(cm, std::abs(sc[k].mismatches[i] - sg[k].mismatches[i]));
+        cx = std::max(cx, std::abs(sc[k].max_mismatch - sg[k].max_mismatch));
+    }
+    double dsame = 0.0;
+    for (int i = 0; i < n; ++i) dsame = std::max(dsame, std::abs(rg2.bus_voltages[i] - rg.bus_voltages[i]));
+    std::cout << "capture_counts " << sc.size() << " " << sg.size() << "\ncapture_iteration_index "
+              << idx_ok << "\ncapture_rel_diff " << cv << " " << ci << " " << cs
+              << "\ncapture_mismatch_abs_diff " << cm << " " << cx << " " << m0
+              << "\ncapture_result " << (rg2.iterations == rg.iterations) << " "
+              << (rg2.converged == rg.converged) << " " << dsame << "\n";
+    gnr->clear_iteration_states();
+    std::cout << "capture_cleared " << gnr->get_iteration_states().size() << "\n";
+    gnr->enable_state_capture(false);
+    cbase.enable_state_capture(false);
+
     // LU: Y (duplicate entries summed, since the reference LU treats duplicates inconsistently:
     // last one wins on its dense path, both kept on its sparse path) with a dominant diagonal
     // added; reference CPU LU vs plugin LU

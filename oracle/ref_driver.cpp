@@ -173,6 +173,50 @@ int gapref_solve(gapref_net const* n, double tol, int max_iter, double base_powe
     }
 }
 
+// The same solve with iteration-state capture on (IPowerFlowSolver::enable_state_capture,
+// cpu_newton_raphson.cpp:95-149): per captured iteration k < cap, max_mis[k] and the voltages
+// v_states[k][n_bus] (re, im), currents i_states and power injections s_states likewise (each
+// nullable).  Returns the number of states captured, or -1 when the solve throws.
+int gapref_solve_states(gapref_net const* n, double tol, int max_iter, double base_power,
+                        int cap, double* max_mis, double* v_states, double* i_states,
+                        double* s_states) {
+    gapref_quiet();
+    try {
+        auto net = to_network(n);
+        gap::admittance::CPUAdmittanceMatrix builder;
+        auto Y = builder.build_admittance_matrix(net);
+        gap::solver::CPUNewtonRaphson nr;
+        nr.set_lu_solver(std::make_shared<gap::solver::CPULUSolver>());
+        gap::solver::IPowerFlowSolver& base = nr;
+        base.enable_state_capture(true);
+        gap::solver::PowerFlowConfig cfg;
+        cfg.tolerance = tol;
+        cfg.max_iterations = max_iter;
+        cfg.base_power = base_power;
+        cfg.use_flat_start = true;
+        nr.solve_power_flow(net, *Y, cfg);
+        auto const& st = base.get_iteration_states();
+        const int nb = n->n_bus;
+        const int k_n = static_cast<int>(st.size());
+        auto put = [nb](double* dst, int k, std::vector<gap::Complex> const& x) {
+            if (!dst) return;
+            for (int i = 0; i < nb && i < static_cast<int>(x.size()); ++i) {
+                dst[(static_cast<size_t>(k) * nb + i) * 2] = x[i].real();
+                dst[(static_cast<size_t>(k) * nb + i) * 2 + 1] = x[i].imag();
+            }
+        };
+        for (int k = 0; k < k_n && k < cap; ++k) {
+            if (max_mis) max_mis[k] = st[k].max_mismatch;
+            put(v_states, k, st[k].voltages);
+            put(i_states, k, st[k].currents);
+            put(s_states, k, st[k].power_injections);
+        }
+        return k_n;
+    } catch (std::exception const&) {
+        return -1;
+    }
+}
+
 // IPowerFlowSolver::calculate_mismatches (Watts, base 100 MVA) for a given voltage vector,
 // using the reference-built Y-bus.
 int gapref_mismatch(gapref_net const* n, double const* v, int cap, double* out) {

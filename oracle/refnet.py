@@ -125,6 +125,26 @@ def solve(net, tol=1e-8, max_iter=20, base_power=1e6):
                 iterations=int(it.value), final_mismatch=float(fm.value))
 
 
+def solve_states(net, tol=1e-8, max_iter=20, base_power=1e6):
+    """Reference CPUNewtonRaphson with iteration-state capture on: a list, per iteration, of
+    dict(max_mismatch, v, i, s) (complex per-unit vectors over the buses)."""
+    L = lib()
+    s, keep = _pack(net)
+    n = net.n_bus
+    cap = max(int(max_iter), 1)
+    mm = np.zeros(cap, np.float64)
+    vs, cs, ss = (np.zeros((cap, n, 2), np.float64) for _ in range(3))
+    k = L.gapref_solve_states(C.byref(s), C.c_double(tol), C.c_int(max_iter),
+                              C.c_double(base_power), C.c_int(cap), _ptr(mm), _ptr(vs),
+                              _ptr(cs), _ptr(ss))
+    if k < 0:
+        raise RuntimeError("reference solve threw")
+    k = min(k, cap)
+    return [dict(max_mismatch=float(mm[j]), v=vs[j].view(np.complex128)[:, 0].copy(),
+                 i=cs[j].view(np.complex128)[:, 0].copy(),
+                 s=ss[j].view(np.complex128)[:, 0].copy()) for j in range(k)]
+
+
 def mismatch(net, v):
     L = lib()
     s, keep = _pack(net)

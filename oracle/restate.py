@@ -334,14 +334,16 @@ def update_newton(bus_type, v, dx):
 
 
 def nr_solve(net: Network, Y=None, tol=1e-8, max_iter=20, base_power=1e6,
-             policy="reference", jac="reference", s_spec=None, v0=None, history=False):
+             policy="reference", jac="reference", s_spec=None, v0=None, history=False,
+             states=False):
     """CPUNewtonRaphson::solve_power_flow (cpu_newton_raphson.cpp:33-218) with a sparse LU.
 
     policy 'reference' = the reference's damped, clamped update; 'newton' = pure Newton;
     'clamped' = full Newton step with the reference's clamps.
     jac 'reference' = last-wins duplicates and the 1e-12 drop; 'exact' = summed duplicates.
     Y defaults to the reference Y-bus (Siemens).  Returns dict(v, converged, iterations,
-    final_mismatch[, trace])."""
+    final_mismatch[, trace][, states]); states=True records IterationState per iteration as
+    cpu_newton_raphson.cpp:125-149 does (v, i = Y_pu v, s = v conj(i), mismatch, max)."""
     if Y is None:
         Y = ybus_reference(net)
     row_ptr, col_idx, vals = Y
@@ -355,12 +357,18 @@ def nr_solve(net: Network, Y=None, tol=1e-8, max_iter=20, base_power=1e6,
     bt = net.bus_type
     res = dict(converged=False, iterations=0, final_mismatch=0.0)
     trace = []
+    rec = []
     for it in range(max_iter):
         s = power_injections(row_ptr, col_idx, ypu, v)
         d = mismatch(bt, s, s_spec)
         mx = float(np.max(np.abs(d))) if d.size else 0.0
         res["final_mismatch"] = mx
         trace.append(mx)
+        if states:
+            n = len(row_ptr) - 1
+            cur = sp.csr_matrix((ypu, col_idx, row_ptr), shape=(n, n)) @ v
+            rec.append(dict(iteration=it, v=v.copy(), i=cur, s=v * np.conj(cur),
+                            mismatch=d.copy(), max_mismatch=mx))
         if mx < tol:
             res["converged"] = True
             res["iterations"] = it + 1
@@ -383,6 +391,8 @@ def nr_solve(net: Network, Y=None, tol=1e-8, max_iter=20, base_power=1e6,
     res["v"] = v
     if history:
         res["trace"] = trace
+    if states:
+        res["states"] = rec
     return res
 
 

@@ -50,9 +50,18 @@ def save(name, **arrays):
 def ref_all(net, tol=1e-8, max_iter=20, base=1e6):
     rp, ci, va = refnet.ybus(net)
     sol = refnet.solve(net, tol, max_iter, base)
+    # iteration-state capture of the same solve (IterationState per iteration,
+    # cpu_newton_raphson.cpp:125-149): max |mismatch| and V; I = Y V and S = V conj(I) too on
+    # grids of up to 64 buses (they follow from V and Y, so larger grids keep V only)
+    st = refnet.solve_states(net, tol, max_iter, base)
+    cap = dict(cap_max_mis=np.array([x["max_mismatch"] for x in st]),
+               cap_v=np.array([x["v"] for x in st]).reshape(len(st), net.n_bus))
+    if net.n_bus <= 64:
+        cap["cap_i"] = np.array([x["i"] for x in st]).reshape(len(st), net.n_bus)
+        cap["cap_s"] = np.array([x["s"] for x in st]).reshape(len(st), net.n_bus)
     return dict(y_row_ptr=rp, y_col_idx=ci, y_values=va, ref_v=sol["v"],
                 ref_converged=np.int32(sol["converged"]), ref_iterations=np.int32(sol["iterations"]),
-                ref_final_mismatch=np.float64(sol["final_mismatch"]))
+                ref_final_mismatch=np.float64(sol["final_mismatch"]), **cap)
 
 
 def simple_lists_to_network(bus_data, branch_data):

@@ -213,6 +213,85 @@ def test_graph_and_host_loop_agree():
     np.testing.assert_array_equal(outs[0][0], outs[1][0])
 
 
+@pytest.mark.parametrize("name", [n for n in fixture_names("kat_") if n != "kat_update"]
+                         + fixture_names("c0_")[:2] + fixture_names("pgm_")[:4])
+def test_iteration_state_capture_matches_reference(name):
+    """enable_state_capture / get_iteration_states (powerflow_interface.h:83-107): one
+    IterationState per iteration, state by state against the reference's own capture
+    (cpu_newton_raphson.cpp:125-149), and the capturing solve's result equal to the plain
+    solve's."""
+    from gap_b200.api import NewtonRaphson, PowerFlowConfig
+
+    net, d = network_of(name)
+    cfg = PowerFlowConfig(tolerance=1e-8, max_iterations=20, base_power=float(d["base_power"]))
+    Y = (d["y_row_ptr"], d["y_col_idx"], d["y_values"])
+    nr = NewtonRaphson()
+    plain = nr.solve_power_flow(net, Y, cfg)
+    assert nr.get_iteration_states() == []
+    nr.enable_state_capture(True)
+    r = nr.solve_power_flow(net, Y, cfg)
+    st = nr.get_iteration_states()
+    assert (r.converged, r.iterations) == (plain.converged, plain.iterations)
+    np.testing.assert_array_equal(r.bus_voltages, plain.bus_voltages)
+    assert len(st) == r.iterations
+    ref_m = d["cap_max_mis"]
+    assert abs(len(st) - len(ref_m)) <= 1
+    m0 = max(1.0, float(np.max(ref_m)))
+    for k in range(min(len(st), len(ref_m))):
+        assert st[k].iteration == k
+        assert abs(st[k].max_mismatch - ref_m[k]) <= 1e-9 * m0
+        assert st[k].max_mismatch == np.max(np.abs(st[k].mismatches), initial=0.0)
+        assert np.max(np.abs(st[k].voltages - d["cap_v"][k])) < 1e-9
+        if "cap_i" in d:
+            si = max(1.0, float(np.max(np.abs(d["cap_i"][k]))))
+            ss = max(1.0, float(np.max(np.abs(d["cap_s"][k]))))
+            assert np.max(np.abs(st[k].currents - d["cap_i"][k])) <= 1e-9 * si
+            assert np.max(np.abs(st[k].power_injections - d["cap_s"][k])) <= 1e-9 * ss
+    nr.clear_iteration_states()
+    assert nr.get_iteration_states() == []
+
+
+def test_stepped_batch_matches_oracle_states():
+    """gapk_nr_step / gapk_nr_get_state on a lane-interleaved FP64 batch: every scenario's
+    recorded states against the oracle's, and the outputs equal to gapk_nr_solve's."""
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.feeder_grid(1)
+    zb = net.u_rated[0] ** 2 / 1e6
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type)
+    S = 6
+    rng = np.random.default_rng(5)
+    s0 = net.specified_power(1e6)
+    sc = s0[None, :] * rng.uniform(0.6, 1.3, size=(S, 1))
+    s = torch.as_tensor(sc, device="cuda")
+    b = NRBatch(plan, S, precision="fp64", lanes=4)
+    ref = b.solve(y, s, tol=1e-8, max_iter=20)
+    r, states = b.solve_captured(y, s, tol=1e-8, max_iter=20)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(r.v.cpu().numpy(), ref.v.cpu().numpy())
+    np.testing.assert_array_equal(r.iterations.cpu().numpy(), ref.iterations.cpu().numpy())
+    its = r.iterations.cpu().numpy()
+    assert len(states) == int(its.max())
+    rp, ci, va = restate.ybus_reference(net)
+    for q in range(S):
+        o = restate.nr_solve(net, Y=(rp, ci, va), tol=1e-8, max_iter=20, base_power=1e6,
+                             s_spec=sc[q], states=True)
+        assert abs(o["iterations"] - int(its[q])) <= 1
+        m0 = max(1.0, o["states"][0]["max_mismatch"])
+        for k in range(min(int(its[q]), len(o["states"]))):
+            g, w = states[k], o["states"][k]
+            assert np.max(np.abs(g["v"][q].cpu().numpy() - w["v"])) < 1e-9
+            assert np.max(np.abs(g["mismatch"][q].cpu().numpy() - w["mismatch"])) <= 1e-9 * m0
+            si = max(1.0, float(np.max(np.abs(w["i"]))))
+            assert np.max(np.abs(g["i"][q].cpu().numpy() - w["i"])) <= 1e-9 * si
+            assert np.max(np.abs(g["s"][q].cpu().numpy() - w["s"])) <= 1e-9 * si
+
+
 def test_max_iterations_semantics():
     """max_iterations reached: iterations == max, not converged, final mismatch from the last
     evaluation (cpu_newton_raphson.cpp:100-174)."""

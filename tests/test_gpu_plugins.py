@@ -74,6 +74,17 @@ def test_plugins_drop_in_against_reference_backends(name, tmp_path):
     assert o["mismatch_sizes"][0] == o["mismatch_sizes"][1]
     dm, sm = o["mismatch_max_abs_diff"]
     assert dm <= 1e-9 * sm + 1e-6
+    # iteration-state capture: one state per iteration on both sides, the same states along
+    # the trajectory, and the capturing solve's result equal to the plain one
+    nc, ng = o["capture_counts"]
+    assert nc == ic and ng == ig
+    assert o["capture_iteration_index"] == [1]
+    if cc:
+        assert max(o["capture_rel_diff"]) < 1e-9
+        cm, cx, m0 = o["capture_mismatch_abs_diff"]
+        assert cm <= 1e-9 * max(m0, 1.0) and cx <= 1e-9 * max(m0, 1.0)
+    assert o["capture_result"] == [1, 1, 0.0]
+    assert o["capture_cleared"] == [0]
     assert o["lu_factorized"] == [1, 1, 1]
     assert o["lu_rel_diff"][0] < 1e-10
     assert o["lu_bad_rhs_throws"] == [1]

@@ -32,6 +32,30 @@ def test_nr_restatement_matches_reference(name):
         assert np.max(np.abs(np.angle(r["v"]) - np.angle(d["ref_v"]))) < 1e-10
 
 
+@pytest.mark.parametrize("name", FIX)
+def test_iteration_states_match_reference_capture(name):
+    """IterationState per iteration (cpu_newton_raphson.cpp:125-149, captured from the
+    reference by tests/golden/make_golden.py): the restatement's trajectory state by state."""
+    net, d = network_of(name)
+    r = restate.nr_solve(net, tol=1e-8, max_iter=20, base_power=float(d["base_power"]),
+                         states=True)
+    st = r["states"]
+    ref_m = d["cap_max_mis"]
+    assert len(ref_m) == int(d["ref_iterations"])
+    assert len(st) == r["iterations"]
+    m0 = max(1.0, float(np.max(ref_m)))
+    for k in range(min(len(st), len(ref_m))):
+        assert st[k]["iteration"] == k
+        assert abs(st[k]["max_mismatch"] - ref_m[k]) <= 1e-10 * m0
+        assert np.max(np.abs(st[k]["v"] - d["cap_v"][k])) < 1e-10
+        assert st[k]["max_mismatch"] == np.max(np.abs(st[k]["mismatch"]), initial=0.0)
+        if "cap_i" in d:
+            si = max(1.0, float(np.max(np.abs(d["cap_i"][k]))))
+            ss = max(1.0, float(np.max(np.abs(d["cap_s"][k]))))
+            assert np.max(np.abs(st[k]["i"] - d["cap_i"][k])) <= 1e-10 * si
+            assert np.max(np.abs(st[k]["s"] - d["cap_s"][k])) <= 1e-10 * ss
+
+
 @pytest.mark.parametrize("name", fixture_names("pgm_"))
 def test_reference_and_restatement_vs_power_grid_model(name):
     """The reference's own acceptance criterion (tests/pgm_validation/test_pgm_validation.py:38-43):
