@@ -353,6 +353,21 @@ def run_ours(args, rank, world, device):
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
         kt[name] = sorted(ts)[1]
+    # per-level latency of the level-scheduled kernels (%globaltimer stamps, one launch each)
+    lt = batch.level_trace(y, s_dev, v_init=v_dev)
+
+    def level_summary(d):
+        med = np.median(d["level_us"], axis=0)  # per level, median over lane groups
+        return {"total_us": float(np.median(d["total_us"])),
+                "per_level_us_median": float(np.median(med)) if med.size else 0.0,
+                "slowest_level_us": float(med.max()) if med.size else 0.0}
+
+    lu_levels = {"critical_path_levels": info["n_levels"], "dense_tail_order": 2 * info["n_tail"],
+                 "max_level_width": info["max_level_width"],
+                 "factor_sparse": level_summary(lt["factor"]),
+                 "solve_fwd": level_summary(lt["forward"]),
+                 "solve_bwd": level_summary(lt["backward"]),
+                 "source": "%globaltimer stamps at each level barrier, median over lane groups"}
     per_iter = {"mismatch": 1, "jacobian": 1, "factor_sparse": 1, "schur": 1, "dense_lu": 1,
                 "solve_fwd": 2, "dense_solve": 2, "solve_bwd": 2, "update": 1}
     if info["n_tail"] == 0:
@@ -425,7 +440,7 @@ def run_ours(args, rank, world, device):
                          if traffic else None,
                          "fp32_fma_tflops": fma_tflops,
                          "launch_ms": kt[dom], "peak_source": "measured" if peaks else "fallback"},
-            "kernel_ms": kt, "kernel_share_ms_per_iter": share,
+            "kernel_ms": kt, "kernel_share_ms_per_iter": share, "lu_levels": lu_levels,
             "plain_fp64_single": plain,
             "batched_over_plain_fp64": value / plain["value"] if plain["value"] else None,
             "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": gpu_launches,

@@ -33,7 +33,8 @@ EXPORTS = [
     "gapk_nr_stage_load", "gapk_nr_stage_mismatch", "gapk_nr_stage_jacobian",
     "gapk_nr_stage_factor", "gapk_nr_stage_solve", "gapk_nr_stage_get_correction",
     "gapk_nr_stage_get_mismatch", "gapk_nr_stage_kernel", "gapk_nr_solve_noalloc",
-    "gapk_nr_step", "gapk_nr_get_state", "gapk_nr_get_outputs",
+    "gapk_nr_step", "gapk_nr_get_state", "gapk_nr_get_outputs", "gapk_nr_level_trace_size",
+    "gapk_nr_set_level_trace",
     "gapk_splu_create", "gapk_splu_destroy", "gapk_splu_size", "gapk_splu_factorize",
     "gapk_splu_solve", "gapk_nr_adjoint", "gapk_nr_adjoint_branch", "gapk_branch_flows",
 ]
@@ -89,6 +90,8 @@ def lib():
         L.gapk_last_error.restype = C.c_char_p
         L.gapk_nr_plan_export.restype = C.c_int64
         L.gapk_nr_batch_device_bytes.restype = C.c_int64
+        L.gapk_nr_level_trace_size.restype = C.c_int64
+        L.gapk_nr_set_level_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         for name in ("gapk_ybus_create", "gapk_nr_plan_create", "gapk_nr_batch_create"):
             getattr(L, name).restype = C.c_int
         L.gapk_ybus_assemble.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64,

@@ -897,6 +897,29 @@ int gapk_nr_get_state(gapk_nr_batch b, double* d_v, double* d_i, double* d_s, vo
     return check_launch();
 }
 
+int64_t gapk_nr_level_trace_size(gapk_nr_batch b) {
+    if (!b) return 0;
+    return 3 * static_cast<int64_t>(b->G) * (b->plan->h.n_levels + 2);
+}
+
+int gapk_nr_set_level_trace(gapk_nr_batch b, unsigned long long* d_stamps, int64_t n_stamps) {
+    if (!b || (d_stamps && n_stamps < gapk_nr_level_trace_size(b))) {
+        set_error("gapk_nr_set_level_trace: null batch or stamp buffer too small");
+        return GAPK_EINVAL;
+    }
+    b->dev.lvl_ts = d_stamps;
+    // the solve graph holds the previous setting: rebuild it on the next gapk_nr_solve
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return GAPK_OK;
+}
+
 int gapk_nr_get_outputs(gapk_nr_batch b, const gapk_nr_outputs* out, void* stream) {
     if (!b || !out) {
         set_error("gapk_nr_get_outputs: bad arguments");

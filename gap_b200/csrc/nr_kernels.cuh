@@ -80,7 +80,23 @@ struct BatchDev {
     int* grefine;     // [G] refinement pass runs for the group this iteration (null: always)
     int* gfactor;     // [G] the group refactorises this iteration (null: always); else the
                       //     previous factors precondition the refined solve
+    unsigned long long* lvl_ts;  // level trace (null: off): %globaltimer stamps
+                                 // [3 kernels: factor, forward, backward][G][n_levels + 2]
 };
+
+// nanosecond clock of the level trace (PTX special register %globaltimer)
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// stamp j of kernel `which` for group g: 0 = start, 1 + h = level h done (in execution order),
+// n_levels + 1 = end; one thread per CTA, after a barrier
+__device__ __forceinline__ void lvl_stamp(BatchDev const& B, int n_levels, int which, int g,
+                                          int j) {
+    if (threadIdx.x == 0)
+        B.lvl_ts[((size_t)which * B.n_groups + g) * (n_levels + 2) + j] = gtimer();
+}
 
 // ---------------------------------------------------------------------------------------
 // load: interleave inputs, flat start, reset state
@@ -384,6 +400,7 @@ __global__ void k_factor(PlanDev P, BatchDev B) {
     const int lane = threadIdx.x % SW;
     const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
     bool bad = false;
+    if (B.lvl_ts) lvl_stamp(B, P.n_levels, 0, g, 0);
     for (int h = 0; h < P.n_levels; ++h) {
         const int ta = P.fa_ptr[h], tb = P.fa_ptr[h + 1];
         for (int t = ta + e0; t < tb; t += ne) {
@@ -411,7 +428,9 @@ __global__ void k_factor(PlanDev P, BatchDev B) {
             }
             __syncthreads();
         }
+        if (B.lvl_ts) lvl_stamp(B, P.n_levels, 0, g, h + 1);
     }
+    if (B.lvl_ts) lvl_stamp(B, P.n_levels, 0, g, P.n_levels + 1);
     if (bad) B.singular[g * SW + lane] = 1;
 }
 
@@ -1020,6 +1039,7 @@ __global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ r
     const double2* R = rhs + (size_t)g * P.nb * SW;
     const int lane = threadIdx.x % SW;
     const int e0 = threadIdx.x / SW, ne = blockDim.x / SW;
+    if (B.lvl_ts) lvl_stamp(B, P.n_levels, 1, g, 0);
     for (int h = 0; h < P.n_levels; ++h) {
         const int lb = P.level_ptr[h], c = P.level_ptr[h + 1] - lb;
         const int s = split_factor(c, ne);
@@ -1053,6 +1073,7 @@ __global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ r
             }
         }
         __syncthreads();
+        if (B.lvl_ts) lvl_stamp(B, P.n_levels, 1, g, h + 1);
     }
     for (int k = P.ns + e0; k < P.nb; k += ne) {
         const double2 b = R[(size_t)k * SW + lane];
@@ -1063,6 +1084,10 @@ __global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ r
             msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
         }
         stv(X + (size_t)k * SW + lane, acc);
+    }
+    if (B.lvl_ts) {
+        __syncthreads();
+        lvl_stamp(B, P.n_levels, 1, g, P.n_levels + 1);
     }
 }
 
@@ -1088,6 +1113,7 @@ __global__ void k_solve_bwd(PlanDev P, BatchDev B, double2* out, int accumulate)
             *o = make_double2((double)x.x, (double)x.y);
         }
     };
+    if (B.lvl_ts) lvl_stamp(B, P.n_levels, 2, g, 0);
     for (int h = P.n_levels - 1; h >= 0; --h) {
         const int lb = P.level_ptr[h], c = P.level_ptr[h + 1] - lb;
         const int s = split_factor(c, ne);
@@ -1120,7 +1146,9 @@ __global__ void k_solve_bwd(PlanDev P, BatchDev B, double2* out, int accumulate)
             }
         }
         __syncthreads();
+        if (B.lvl_ts) lvl_stamp(B, P.n_levels, 2, g, P.n_levels - h);
     }
+    if (B.lvl_ts) lvl_stamp(B, P.n_levels, 2, g, P.n_levels + 1);
 }
 
 // refinement residual: res = rhs - J dx with the FP64 Jacobian blocks

@@ -322,6 +322,34 @@ class NRBatch:
         N.check(N.lib().gapk_nr_stage_kernel(self._h, self.KERNELS.index(name),
                                              _stream_ptr(stream)))
 
+    def level_trace(self, y, s_spec, v_init=None, u_pu=None, stream=None):
+        """Per-level latency of the level-scheduled kernels at the state (y, s_spec, v_init):
+        one mismatch and Jacobian, then the sparse factorisation, Schur gather, dense LU and
+        the three solves, each launched once with the level trace on
+        (gapk_nr_set_level_trace).  Returns, per kernel ("factor", "forward", "backward"),
+        dict(stamps = %globaltimer ns [n_groups, n_levels + 2], level_us = duration of each
+        level in execution order [n_groups, n_levels], total_us [n_groups])."""
+        torch = _torch()
+        L = N.lib()
+        n = int(L.gapk_nr_level_trace_size(self._h))
+        buf = torch.zeros(n, dtype=torch.int64, device=s_spec.device)
+        self.stage_load(y, s_spec, v_init=v_init, u_pu=u_pu, stream=stream)
+        self.kernel("mismatch", stream)
+        self.kernel("jacobian", stream)
+        N.check(L.gapk_nr_set_level_trace(self._h, _dptr(buf), n))
+        try:
+            for k in ("factor_sparse", "schur", "dense_lu", "solve_fwd", "dense_solve",
+                      "solve_bwd"):
+                self.kernel(k, stream)
+            torch.cuda.synchronize()
+        finally:
+            N.check(L.gapk_nr_set_level_trace(self._h, None, 0))
+        lv = self.plan.info["n_levels"]
+        ts = buf.cpu().numpy().reshape(3, -1, lv + 2)
+        return {name: dict(stamps=ts[i], level_us=np.diff(ts[i][:, :lv + 1], axis=1) / 1e3,
+                           total_us=(ts[i][:, -1] - ts[i][:, 0]) / 1e3)
+                for i, name in enumerate(("factor", "forward", "backward"))}
+
     def correction(self, stream=None):
         torch = _torch()
         nv = self.plan.info["n_vars"]

@@ -242,6 +242,18 @@ int gapk_nr_step(gapk_nr_batch b, int* h_active, void* stream);
 int gapk_nr_get_state(gapk_nr_batch b, double* d_v, double* d_i, double* d_s, void* stream);
 int gapk_nr_get_outputs(gapk_nr_batch b, const gapk_nr_outputs* out, void* stream);
 
+/* ==== Level trace (per-level latency of the level-scheduled kernels) ======================
+ * No counterpart in the reference (its only timers are host std::chrono phase totals,
+ * src/solver/powerflow/cpu/cpu_newton_raphson.cpp:23-30,181-206).  With d_stamps set (device
+ * memory of gapk_nr_level_trace_size(b) uint64 values), the sparse factorisation and the
+ * sparse forward and backward solves write %globaltimer stamps (ns) into
+ * [kernel: 0 factor, 1 forward, 2 backward][lane group][j], j = 0 at the kernel's start,
+ * 1 + i when the i-th level in execution order is done, n_levels + 1 at the end; one CTA per
+ * lane group writes its own row.  NULL switches the trace off.  Changing the setting makes the
+ * next gapk_nr_solve rebuild its graph. */
+int64_t gapk_nr_level_trace_size(gapk_nr_batch b);
+int gapk_nr_set_level_trace(gapk_nr_batch b, unsigned long long* d_stamps, int64_t n_stamps);
+
 /* ==== Adjoint (gradients through the converged state; no counterpart in the reference) ====
  * With the batch holding a converged state (after gapk_nr_solve, or gapk_nr_stage_load with
  * the solution as d_v_init), refactorises the Jacobian at that state and solves

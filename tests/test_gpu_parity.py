@@ -349,6 +349,48 @@ def test_dense_tail_correction_matches_sparse_solve(precision, lanes, dense_min)
         assert np.max(np.abs(dx[s] - xr)) <= tol * np.max(np.abs(xr))
 
 
+def test_level_trace_stamps_and_unchanged_results():
+    """gapk_nr_set_level_trace: per-group stamps ordered in time for the factorisation and both
+    solves, and the correction computed with the trace on equal to the one computed without."""
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.transmission_grid(9, n=4000)
+    base = 1e8
+    zb = net.u_rated[0] ** 2 / base
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
+    assert plan.info["n_tail"] > 50
+    S = 16
+    rng = np.random.default_rng(3)
+    v = torch.as_tensor(np.stack([synth.dc_start(net, base) * np.exp(1j * rng.normal(0, 0.01,
+                                                                                     net.n_bus))
+                                  for _ in range(S)]), device="cuda")
+    s = torch.as_tensor(np.repeat(net.specified_power(base)[None], S, axis=0), device="cuda")
+    b = NRBatch(plan, S, precision="fp32", lanes=8)
+    b.stage_load(y, s, v_init=v)
+    for st in ("mismatch", "jacobian", "factor", "solve"):
+        b.stage(st)
+    dx0 = b.correction()
+    lt = b.level_trace(y, s, v_init=v)
+    dx1 = b.correction()
+    assert torch.equal(dx0, dx1)
+    L = plan.info["n_levels"]
+    for k in ("factor", "forward", "backward"):
+        st = lt[k]["stamps"]
+        assert st.shape == (2, L + 2)
+        assert (st[:, 0] > 0).all() and (np.diff(st, axis=1) >= 0).all()
+        assert lt[k]["level_us"].shape == (2, L)
+        assert (lt[k]["total_us"] > 0).all() and (lt[k]["total_us"] < 1e5).all()
+    # trace off afterwards: a plain solve is unaffected and writes no stamps
+    r = b.solve(y, s, v_init=v, tol=1e-8, max_iter=20, policy="newton", refine=1)
+    torch.cuda.synchronize()
+    assert bool((r.status == 0).all())
+
+
 def _csr(A):
     rows, cols = np.nonzero(A)
     rp = np.zeros(A.shape[0] + 1, np.int32)
