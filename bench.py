@@ -368,6 +368,15 @@ def run_ours(args, rank, world, device):
                  "solve_fwd": level_summary(lt["forward"]),
                  "solve_bwd": level_summary(lt["backward"]),
                  "source": "%globaltimer stamps at each level barrier, median over lane groups"}
+    if "dense" in lt:
+        ph = np.median(lt["dense"]["phase_us"], axis=0)  # [panels, 3], median over scenarios
+        st = lt["dense"]["stamps"]
+        lu_levels["dense_lu"] = {
+            "panels": int(ph.shape[0]), "total_us": float(np.median(st[:, -1] - st[:, 0]) / 1e3),
+            "diagonal_blocks_us": float(ph[:, 0].sum()), "l21_u12_solves_us": float(ph[:, 1].sum()),
+            "trailing_updates_us": float(ph[:, 2].sum()),
+            "source": "per-panel stamps of one CTA (one scenario), median over scenarios; "
+                      "CTAs run 2 per SM in 3.5 waves"}
     per_iter = {"mismatch": 1, "jacobian": 1, "factor_sparse": 1, "schur": 1, "dense_lu": 1,
                 "solve_fwd": 2, "dense_solve": 2, "solve_bwd": 2, "update": 1}
     if info["n_tail"] == 0:

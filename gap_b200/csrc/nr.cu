@@ -749,6 +749,8 @@ int gapk_nr_batch_destroy(gapk_nr_batch b) {
     return GAPK_OK;
 }
 
+int gapk_nr_batch_lanes(gapk_nr_batch b) { return b ? b->sw : 0; }
+
 int64_t gapk_nr_batch_device_bytes(gapk_nr_batch b) {
     if (!b) return 0;
     int64_t s = 0;
@@ -897,9 +899,25 @@ int gapk_nr_get_state(gapk_nr_batch b, double* d_v, double* d_i, double* d_s, vo
     return check_launch();
 }
 
+static int64_t sparse_trace_size(gapk_nr_batch b) {
+    return 3 * static_cast<int64_t>(b->G) * (b->plan->h.n_levels + 2);
+}
+// the panel trace exists when the one-CTA-per-scenario dense LU factorises the tail
+static int64_t dense_trace_size(gapk_nr_batch b) {
+    const int N = 2 * b->plan->h.n_tail;
+    if (N == 0 || b->dense_split || b->dense_w <= 0) return 0;
+    return static_cast<int64_t>(b->G) * b->sw * (1 + 3 * ((N + b->dense_w - 1) / b->dense_w));
+}
+
 int64_t gapk_nr_level_trace_size(gapk_nr_batch b) {
     if (!b) return 0;
-    return 3 * static_cast<int64_t>(b->G) * (b->plan->h.n_levels + 2);
+    return sparse_trace_size(b) + dense_trace_size(b);
+}
+
+int gapk_nr_dense_trace_panels(gapk_nr_batch b) {
+    if (!b || dense_trace_size(b) == 0) return 0;
+    const int N = 2 * b->plan->h.n_tail;
+    return (N + b->dense_w - 1) / b->dense_w;
 }
 
 int gapk_nr_set_level_trace(gapk_nr_batch b, unsigned long long* d_stamps, int64_t n_stamps) {
@@ -908,6 +926,7 @@ int gapk_nr_set_level_trace(gapk_nr_batch b, unsigned long long* d_stamps, int64
         return GAPK_EINVAL;
     }
     b->dev.lvl_ts = d_stamps;
+    b->dev.dlu_ts = d_stamps && dense_trace_size(b) ? d_stamps + sparse_trace_size(b) : nullptr;
     // the solve graph holds the previous setting: rebuild it on the next gapk_nr_solve
     if (b->exec) {
         cudaGraphExecDestroy(b->exec);

@@ -82,6 +82,9 @@ struct BatchDev {
                       //     previous factors precondition the refined solve
     unsigned long long* lvl_ts;  // level trace (null: off): %globaltimer stamps
                                  // [3 kernels: factor, forward, backward][G][n_levels + 2]
+    unsigned long long* dlu_ts;  // dense-tail panel trace of k_dense_lu (null: off)
+                                 // [G*SW][1 + 3 * panels]: start, then per panel the ends of
+                                 // the diagonal block, the L21/U12 solves, the trailing update
 };
 
 // nanosecond clock of the level trace (PTX special register %globaltimer)
@@ -500,6 +503,10 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
                      : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// Hint: bring the line holding p into L2 (no register result, nothing to wait for).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 
 // Right-looking blocked LU without pivoting of one scenario's N x N tail (row-major, row
 // stride dense_ld(N), in place), panels of W columns (W = 8, 16 or 32; compile time):
@@ -660,6 +667,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchD
     const int tid = threadIdx.x, nt = blockDim.x;
     constexpr int VE = 16 / sizeof(T);
     if (tid == 0) bad = 0;
+    // panel trace stamp j of this scenario (the address is rebuilt from the kernel
+    // parameters at each stamp, so that the trace holds no registers across the loop)
+    auto stamp = [&](int j, bool copy_prev) {
+        if (B.dlu_ts && tid == 0) {
+            unsigned long long* t = B.dlu_ts + (size_t)q * (1 + 3 * ((N + W - 1) / W)) + j;
+            *t = copy_prev ? t[-1] : gtimer();
+        }
+    };
+    stamp(0, false);
     for (int k0 = 0; k0 < N; k0 += W) {
         const int w = min(W, N - k0);
         const int m = N - k0;
@@ -669,6 +685,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchD
             if (dense_diag_block<T, W>(A, ld, k0, w, PT, ld, SL, SD)) bad = 1;
         }
         __syncthreads();
+        stamp(1 + 3 * (k0 / W), false);
         if (n2 > 0) {
             // ---- B: rows of L21 and columns of U12, one per thread at a time
             for (int it = tid; it < 2 * n2; it += nt) {
@@ -680,6 +697,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchD
                 }
             }
             __syncthreads();
+            stamp(2 + 3 * (k0 / W), false);
             // ---- C: trailing update, U12 in double-buffered chunks
             const int nch = (n2 + DCW - 1) / DCW;
             auto stage = [&](int ch, T* buf) {
@@ -704,6 +722,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchD
                 const int ntile = tr8 * tcn;
                 for (int tix = tid; tix < ntile; tix += nt) {
                     const int i0 = W + (tix / tcn) * 8, cc0 = (tix % tcn) * 8;
+                    if (tix + nt < ntile) {
+                        // the thread's next tile goes to L2 while this one computes
+                        const int j0 = W + ((tix + nt) / tcn) * 8, dc0 = ((tix + nt) % tcn) * 8;
+                        const T* pf = A + (size_t)(k0 + j0) * ld + k0 + W + c0 + dc0;
+#pragma unroll
+                        for (int ii = 0; ii < 8; ++ii)
+                            if (j0 + ii < m) prefetch_l2(pf + (size_t)ii * ld);
+                    }
                     T acc[8][8];
 #pragma unroll
                     for (int ii = 0; ii < 8; ++ii) {
@@ -743,7 +769,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchD
                 cp_async_wait_all();
                 __syncthreads();
             }
+        } else {
+            stamp(2 + 3 * (k0 / W), true);
         }
+        stamp(3 + 3 * (k0 / W), false);
     }
     if (tid == 0 && bad) B.singular[q] = 1;
 }

@@ -328,7 +328,9 @@ class NRBatch:
         the three solves, each launched once with the level trace on
         (gapk_nr_set_level_trace).  Returns, per kernel ("factor", "forward", "backward"),
         dict(stamps = %globaltimer ns [n_groups, n_levels + 2], level_us = duration of each
-        level in execution order [n_groups, n_levels], total_us [n_groups])."""
+        level in execution order [n_groups, n_levels], total_us [n_groups]); and, when the
+        one-CTA-per-scenario dense LU runs, "dense": dict(stamps [n_scen, 1 + 3 * panels],
+        phase_us [n_scen, panels, 3] = diagonal block, L21/U12 solves, trailing update)."""
         torch = _torch()
         L = N.lib()
         n = int(L.gapk_nr_level_trace_size(self._h))
@@ -345,10 +347,22 @@ class NRBatch:
         finally:
             N.check(L.gapk_nr_set_level_trace(self._h, None, 0))
         lv = self.plan.info["n_levels"]
-        ts = buf.cpu().numpy().reshape(3, -1, lv + 2)
-        return {name: dict(stamps=ts[i], level_us=np.diff(ts[i][:, :lv + 1], axis=1) / 1e3,
-                           total_us=(ts[i][:, -1] - ts[i][:, 0]) / 1e3)
-                for i, name in enumerate(("factor", "forward", "backward"))}
+        host = buf.cpu().numpy()
+        ns = 3 * (n_groups := self._groups()) * (lv + 2)
+        ts = host[:ns].reshape(3, n_groups, lv + 2)
+        out = {name: dict(stamps=ts[i], level_us=np.diff(ts[i][:, :lv + 1], axis=1) / 1e3,
+                          total_us=(ts[i][:, -1] - ts[i][:, 0]) / 1e3)
+               for i, name in enumerate(("factor", "forward", "backward"))}
+        npan = int(L.gapk_nr_dense_trace_panels(self._h))
+        if npan:
+            d = host[ns:].reshape(-1, 1 + 3 * npan)[:self.n_scen]
+            out["dense"] = dict(stamps=d, phase_us=np.diff(d, axis=1).reshape(-1, npan, 3) / 1e3)
+        return out
+
+    def _groups(self):
+        """Lane groups of the batch: ceil(n_scen / lanes)."""
+        sw = int(N.lib().gapk_nr_batch_lanes(self._h))
+        return -(-self.n_scen // sw)
 
     def correction(self, stream=None):
         torch = _torch()

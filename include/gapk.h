@@ -191,6 +191,8 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
 int gapk_nr_batch_destroy(gapk_nr_batch b);
 /* Device bytes held by the batch. */
 int64_t gapk_nr_batch_device_bytes(gapk_nr_batch b);
+/* Scenarios per lane group (the interleave width the batch was created with, or chose). */
+int gapk_nr_batch_lanes(gapk_nr_batch b);
 
 #define GAPK_POLICY_REFERENCE 0 /* damping 0.9, |dtheta|<=0.15, |d|V||<=0.08, |V| in [0.5,1.5]
                                    (cpu_newton_raphson.cpp:438-504)                         */
@@ -249,9 +251,14 @@ int gapk_nr_get_outputs(gapk_nr_batch b, const gapk_nr_outputs* out, void* strea
  * sparse forward and backward solves write %globaltimer stamps (ns) into
  * [kernel: 0 factor, 1 forward, 2 backward][lane group][j], j = 0 at the kernel's start,
  * 1 + i when the i-th level in execution order is done, n_levels + 1 at the end; one CTA per
- * lane group writes its own row.  NULL switches the trace off.  Changing the setting makes the
- * next gapk_nr_solve rebuild its graph. */
+ * lane group writes its own row.  When the batch factorises its dense tail with the
+ * one-CTA-per-scenario kernel, a panel trace follows: [scenario (padded to whole lane
+ * groups)][1 + 3 * panels], the kernel's start, then per panel of gapk_nr_dense_trace_panels
+ * the ends of the diagonal-block factorisation, of the L21 / U12 solves and of the trailing
+ * update.  NULL switches the trace off.  Changing the setting makes the next gapk_nr_solve
+ * rebuild its graph. */
 int64_t gapk_nr_level_trace_size(gapk_nr_batch b);
+int gapk_nr_dense_trace_panels(gapk_nr_batch b);
 int gapk_nr_set_level_trace(gapk_nr_batch b, unsigned long long* d_stamps, int64_t n_stamps);
 
 /* ==== Adjoint (gradients through the converged state; no counterpart in the reference) ====

@@ -364,11 +364,11 @@ def test_level_trace_stamps_and_unchanged_results():
                     torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
     plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
     assert plan.info["n_tail"] > 50
-    S = 16
+    S = 304  # >= 2 per SM: the one-CTA-per-scenario dense LU, which writes the panel trace
     rng = np.random.default_rng(3)
-    v = torch.as_tensor(np.stack([synth.dc_start(net, base) * np.exp(1j * rng.normal(0, 0.01,
-                                                                                     net.n_bus))
-                                  for _ in range(S)]), device="cuda")
+    v0 = synth.dc_start(net, base)
+    v = torch.as_tensor(v0[None] * np.exp(1j * rng.normal(0, 0.01, (S, net.n_bus))),
+                        device="cuda")
     s = torch.as_tensor(np.repeat(net.specified_power(base)[None], S, axis=0), device="cuda")
     b = NRBatch(plan, S, precision="fp32", lanes=8)
     b.stage_load(y, s, v_init=v)
@@ -381,10 +381,15 @@ def test_level_trace_stamps_and_unchanged_results():
     L = plan.info["n_levels"]
     for k in ("factor", "forward", "backward"):
         st = lt[k]["stamps"]
-        assert st.shape == (2, L + 2)
+        assert st.shape == (S // 8, L + 2)
         assert (st[:, 0] > 0).all() and (np.diff(st, axis=1) >= 0).all()
-        assert lt[k]["level_us"].shape == (2, L)
+        assert lt[k]["level_us"].shape == (S // 8, L)
         assert (lt[k]["total_us"] > 0).all() and (lt[k]["total_us"] < 1e5).all()
+    d = lt["dense"]["stamps"]
+    npan = -(-2 * plan.info["n_tail"] // 32)
+    assert d.shape == (S, 1 + 3 * npan)
+    assert (d[:, 0] > 0).all() and (np.diff(d, axis=1) >= 0).all()
+    assert lt["dense"]["phase_us"].shape == (S, npan, 3)
     # trace off afterwards: a plain solve is unaffected and writes no stamps
     r = b.solve(y, s, v_init=v, tol=1e-8, max_iter=20, policy="newton", refine=1)
     torch.cuda.synchronize()
