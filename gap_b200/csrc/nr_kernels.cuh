@@ -406,13 +406,31 @@ __global__ void k_factor(PlanDev P, BatchDev B) {
     if (B.lvl_ts) lvl_stamp(B, P.n_levels, 0, g, 0);
     for (int h = 0; h < P.n_levels; ++h) {
         const int ta = P.fa_ptr[h], tb = P.fa_ptr[h + 1];
-        for (int t = ta + e0; t < tb; t += ne) {
+        // two targets per worker at a time (targets of one level are independent), so that
+        // their gathers overlap in memory
+        for (int t = ta + e0; t < tb; t += 2 * ne) {
+            const bool two = t + ne < tb;
             const int4 tg = P.targets[t];
+            const int4 tg2 = two ? P.targets[t + ne] : make_int4(0, 0, 0, 0);
             Blk<T> acc = (tg.w & 2) ? ldb(F + (size_t)tg.x * SW + lane) : Blk<T>{0, 0, 0, 0};
+            Blk<T> acc2 = (tg2.w & 2) ? ldb(F + (size_t)tg2.x * SW + lane) : Blk<T>{0, 0, 0, 0};
+            const int nb = min(tg.z - tg.y, tg2.z - tg2.y);
+#pragma unroll 2
+            for (int i = 0; i < nb; ++i) {
+                const int2 pr = P.pairs[tg.y + i];
+                const int2 pr2 = P.pairs[tg2.y + i];
+                msub(acc, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
+                msub(acc2, ldb(F + (size_t)pr2.x * SW + lane), ldb(F + (size_t)pr2.y * SW + lane));
+            }
 #pragma unroll 4
-            for (int p = tg.y; p < tg.z; ++p) {
+            for (int p = tg.y + nb; p < tg.z; ++p) {
                 const int2 pr = P.pairs[p];
                 msub(acc, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
+            }
+#pragma unroll 4
+            for (int p = tg2.y + nb; p < tg2.z; ++p) {
+                const int2 pr = P.pairs[p];
+                msub(acc2, ldb(F + (size_t)pr.x * SW + lane), ldb(F + (size_t)pr.y * SW + lane));
             }
             if (tg.w & 1) {
                 bool ok;
@@ -420,6 +438,14 @@ __global__ void k_factor(PlanDev P, BatchDev B) {
                 bad |= !ok;
             }
             stb(F + (size_t)tg.x * SW + lane, acc);
+            if (two) {
+                if (tg2.w & 1) {
+                    bool ok;
+                    acc2 = inv2(acc2, ok);
+                    bad |= !ok;
+                }
+                stb(F + (size_t)tg2.x * SW + lane, acc2);
+            }
         }
         __syncthreads();
         const int sa = P.fb_ptr[h], sb = P.fb_ptr[h + 1];
@@ -1073,16 +1099,36 @@ __global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ r
         const int lb = P.level_ptr[h], c = P.level_ptr[h + 1] - lb;
         const int s = split_factor(c, ne);
         if (s == 1) {
-            for (int t = lb + e0; t < lb + c; t += ne) {
+            // two nodes per worker at a time (nodes of one level are independent)
+            for (int t = lb + e0; t < lb + c; t += 2 * ne) {
+                const bool two = t + ne < lb + c;
                 const int k = P.level_nodes[t];
+                const int k2 = two ? P.level_nodes[t + ne] : k;
                 const double2 b = R[(size_t)k * SW + lane];
-                Vec2<T> acc = {(T)b.x, (T)b.y};
+                const double2 b2 = R[(size_t)k2 * SW + lane];
+                Vec2<T> acc = {(T)b.x, (T)b.y}, acc2 = {(T)b2.x, (T)b2.y};
+                const int qa = P.rptr[k], qe = P.rptr[k + 1];
+                const int qa2 = two ? P.rptr[k2] : 0, qe2 = two ? P.rptr[k2 + 1] : 0;
+                const int nb = min(qe - qa, qe2 - qa2);
+#pragma unroll 2
+                for (int i = 0; i < nb; ++i) {
+                    const int2 r = P.rlist[qa + i];
+                    const int2 r2 = P.rlist[qa2 + i];
+                    msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
+                    msubv(acc2, ldb(F + (size_t)r2.x * SW + lane), ldv(X + (size_t)r2.y * SW + lane));
+                }
 #pragma unroll 4
-                for (int q = P.rptr[k]; q < P.rptr[k + 1]; ++q) {
+                for (int q = qa + nb; q < qe; ++q) {
                     const int2 r = P.rlist[q];
                     msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
                 }
+#pragma unroll 4
+                for (int q = qa2 + nb; q < qe2; ++q) {
+                    const int2 r = P.rlist[q];
+                    msubv(acc2, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
+                }
                 stv(X + (size_t)k * SW + lane, acc);
+                if (two) stv(X + (size_t)k2 * SW + lane, acc2);
             }
         } else {
             const int j = e0 / s, sub = e0 % s;
@@ -1104,15 +1150,27 @@ __global__ void k_solve_fwd(PlanDev P, BatchDev B, const double2* __restrict__ r
         __syncthreads();
         if (B.lvl_ts) lvl_stamp(B, P.n_levels, 1, g, h + 1);
     }
-    for (int k = P.ns + e0; k < P.nb; k += ne) {
-        const double2 b = R[(size_t)k * SW + lane];
-        Vec2<T> acc = {(T)b.x, (T)b.y};
+    {
+        // tail rows gather long sparse rows: 4 sub-slots per row (a shuffle reduction within
+        // the warp, 4 <= 32 / SW), rounds uniform across the block
+        constexpr int TS = 4;
+        const int sub = e0 % TS, per = ne / TS;
+        for (int base = P.ns; base < P.nb; base += per) {
+            const int k = base + e0 / TS;
+            Vec2<T> acc = {T(0), T(0)};
+            if (k < P.nb) {
 #pragma unroll 4
-        for (int q = P.rptr[k]; q < P.rptr[k + 1]; ++q) {
-            const int2 r = P.rlist[q];
-            msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
+                for (int q = P.rptr[k] + sub; q < P.rptr[k + 1]; q += TS) {
+                    const int2 r = P.rlist[q];
+                    msubv(acc, ldb(F + (size_t)r.x * SW + lane), ldv(X + (size_t)r.y * SW + lane));
+                }
+            }
+            acc = split_reduce<T, SW>(acc, TS, sub, 0, lane, red);
+            if (k < P.nb && sub == 0) {
+                const double2 b = R[(size_t)k * SW + lane];
+                stv(X + (size_t)k * SW + lane, Vec2<T>{(T)b.x + acc.x, (T)b.y + acc.y});
+            }
         }
-        stv(X + (size_t)k * SW + lane, acc);
     }
     if (B.lvl_ts) {
         __syncthreads();
@@ -1147,15 +1205,35 @@ __global__ void k_solve_bwd(PlanDev P, BatchDev B, double2* out, int accumulate)
         const int lb = P.level_ptr[h], c = P.level_ptr[h + 1] - lb;
         const int s = split_factor(c, ne);
         if (s == 1) {
-            for (int t = lb + e0; t < lb + c; t += ne) {
+            // two nodes per worker at a time (nodes of one level are independent)
+            for (int t = lb + e0; t < lb + c; t += 2 * ne) {
+                const bool two = t + ne < lb + c;
                 const int k = P.level_nodes[t];
+                const int k2 = two ? P.level_nodes[t + ne] : k;
                 Vec2<T> acc = ldv(X + (size_t)k * SW + lane);
+                Vec2<T> acc2 = ldv(X + (size_t)k2 * SW + lane);
+                const int pa = P.lptr[k], pe = P.lptr[k + 1];
+                const int pa2 = two ? P.lptr[k2] : 0, pe2 = two ? P.lptr[k2 + 1] : 0;
+                const int nb = min(pe - pa, pe2 - pa2);
+#pragma unroll 2
+                for (int i = 0; i < nb; ++i) {
+                    msubv(acc, ldb(F + (size_t)(Ub + pa + i) * SW + lane),
+                          ldv(X + (size_t)P.lidx[pa + i] * SW + lane));
+                    msubv(acc2, ldb(F + (size_t)(Ub + pa2 + i) * SW + lane),
+                          ldv(X + (size_t)P.lidx[pa2 + i] * SW + lane));
+                }
 #pragma unroll 4
-                for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) {
+                for (int p = pa + nb; p < pe; ++p) {
                     msubv(acc, ldb(F + (size_t)(Ub + p) * SW + lane),
                           ldv(X + (size_t)P.lidx[p] * SW + lane));
                 }
+#pragma unroll 4
+                for (int p = pa2 + nb; p < pe2; ++p) {
+                    msubv(acc2, ldb(F + (size_t)(Ub + p) * SW + lane),
+                          ldv(X + (size_t)P.lidx[p] * SW + lane));
+                }
                 finish(k, acc);
+                if (two) finish(k2, acc2);
             }
         } else {
             const int j = e0 / s, sub = e0 % s;
