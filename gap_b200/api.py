@@ -185,10 +185,14 @@ class NewtonRaphson:
             r = batch.solve(y, s, **kw)
             torch.cuda.synchronize()
         st = int(r.status[0].item())
+        # bus_injections, which the reference declares but never fills: S = V conj(Y V) at
+        # the final voltages, per unit of base_power like bus_voltages
+        _, _, s_bus = batch.state()
         return PowerFlowResult(converged=st == N.SCEN_CONVERGED,
                                iterations=int(r.iterations[0].item()),
                                final_mismatch=float(r.final_mismatch[0].item()),
-                               bus_voltages=r.v[0].cpu().numpy(), status=st)
+                               bus_voltages=r.v[0].cpu().numpy(),
+                               bus_injections=s_bus[0].cpu().numpy(), status=st)
 
     def calculate_mismatches(self, net: Network, bus_voltages, admittance_matrix=None):
         """IPowerFlowSolver::calculate_mismatches: reference equation order, in Watts / var

@@ -84,6 +84,11 @@ class B200NewtonRaphson final : public gap::solver::IPowerFlowSolver {
         res.converged = st == GAPK_SCEN_CONVERGED;
         res.iterations = it;
         res.final_mismatch = fm;
+        // bus_injections (declared by powerflow_interface.h:37-43, never filled by the
+        // reference): S = V conj(Y V) at the final voltages, per unit like bus_voltages
+        double* ds = static_cast<double*>(d_sb_.ensure(static_cast<size_t>(n) * 16));
+        check(gapk_nr_get_state(batch_, nullptr, nullptr, ds, nullptr), "gapk_nr_get_state");
+        d_sb_.download(res.bus_injections, n);
         return res;
     }
 
@@ -217,7 +222,7 @@ class B200NewtonRaphson final : public gap::solver::IPowerFlowSolver {
     std::vector<int> bt_, rp_, ci_;
     bool capture_ = false;
     std::vector<gap::solver::IterationState> states_;
-    DeviceBuffer d_y_, d_s_, d_u_, d_v_, d_vo_, d_it_, d_st_, d_fm_, d_f_, d_cap_;
+    DeviceBuffer d_y_, d_s_, d_u_, d_v_, d_vo_, d_it_, d_st_, d_fm_, d_f_, d_cap_, d_sb_;
 };
 
 }  // namespace gapb200

@@ -322,6 +322,18 @@ class NRBatch:
         N.check(N.lib().gapk_nr_stage_kernel(self._h, self.KERNELS.index(name),
                                              _stream_ptr(stream)))
 
+    def state(self, stream=None):
+        """The batch's current state (after solve(): the solution), per unit, complex128
+        [n_scen, n_bus] each: V, the current injections I = Y V and the power injections
+        S = V conj(I) (gapk_nr_get_state)."""
+        torch = _torch()
+        n = self.plan.info["n_bus"]
+        v, i, s = (torch.empty((self.n_scen, n), dtype=torch.complex128, device="cuda")
+                   for _ in range(3))
+        N.check(N.lib().gapk_nr_get_state(self._h, _dptr(v), _dptr(i), _dptr(s),
+                                          _stream_ptr(stream)))
+        return v, i, s
+
     def level_trace(self, y, s_spec, v_init=None, u_pu=None, stream=None):
         """Per-level latency of the level-scheduled kernels at the state (y, s_spec, v_init):
         one mismatch and Jacobian, then the sparse factorisation, Schur gather, dense LU and

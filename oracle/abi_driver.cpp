@@ -130,6 +130,22 @@ int main(int argc, char** argv) {
         dv = std::max(dv, std::abs(std::abs(rc.bus_voltages[i]) - std::abs(rg.bus_voltages[i])));
         da = std::max(da, std::abs(std::arg(rc.bus_voltages[i]) - std::arg(rg.bus_voltages[i])));
     }
+    // bus_injections of the plugin (the reference leaves it empty) against S = V conj(Y V)
+    // from the reference's Y-bus at the plugin's voltages, per unit
+    double dinj = rg.bus_injections.size() == static_cast<size_t>(n) ? 0.0 : 1e300, sinj = 0.0;
+    if (dinj == 0.0) {
+        const double zb = net.buses[0].u_rated * net.buses[0].u_rated / cfg.base_power;
+        for (int i = 0; i < n; ++i) {
+            Complex cur(0.0, 0.0);
+            for (int p = Yc->row_ptr[i]; p < Yc->row_ptr[i + 1]; ++p)
+                cur += Yc->values[p] * zb * rg.bus_voltages[Yc->col_idx[p]];
+            const Complex sref = rg.bus_voltages[i] * std::conj(cur);
+            dinj = std::max(dinj, std::abs(sref - rg.bus_injections[i]));
+            sinj = std::max(sinj, std::abs(sref));
+        }
+    }
+    std::cout << "nr_bus_injections " << rc.bus_injections.size() << " " << dinj << " " << sinj
+              << "\n";
     std::cout << "nr_converged " << rc.converged << " " << rg.converged << "\nnr_iterations "
               << rc.iterations << " " << rg.iterations << "\nnr_max_dv " << dv << "\nnr_max_dangle "
               << da << "\nnr_final_mismatch " << rc.final_mismatch << " " << rg.final_mismatch

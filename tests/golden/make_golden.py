@@ -136,6 +136,9 @@ def make_pgm(ref_root):
 
             extra["pgm_input_json_z"] = np.frombuffer(zlib.compress(open(inp, "rb").read(), 9),
                                                       np.uint8)
+            # and power-grid-model's whole output dataset, for the PGM writer's tests
+            extra["pgm_output_json_z"] = np.frombuffer(
+                zlib.compress(open(outp, "rb").read(), 9), np.uint8)
         save("pgm_" + case, bus_data=np.asarray(bus_data), branch_data=np.asarray(branch_data),
              base_power=np.float64(net.base_power), pgm_u_pu=pgm_u, pgm_u_angle=pgm_a,
              **sol, **extra)

@@ -96,6 +96,10 @@ def test_nr_fp64_matches_reference(name):
     r = NewtonRaphson().solve_power_flow(net, Y, cfg)
     assert r.converged == bool(d["ref_converged"])
     assert abs(r.iterations - int(d["ref_iterations"])) <= 1
+    # bus_injections (never filled by the reference): S = V conj(Y V) per unit at the result
+    zb = float(net.u_rated[0]) ** 2 / cfg.base_power
+    s_ref = restate.power_injections(Y[0], Y[1], Y[2] * zb, r.bus_voltages)
+    assert np.max(np.abs(r.bus_injections - s_ref)) <= 1e-12 * max(1.0, np.max(np.abs(s_ref)))
     if r.converged:
         assert np.max(np.abs(np.abs(r.bus_voltages) - np.abs(d["ref_v"]))) < 1e-8
         assert np.max(np.abs(np.angle(r.bus_voltages) - np.angle(d["ref_v"]))) < 1e-8

@@ -8,7 +8,7 @@ import zlib
 import numpy as np
 import pytest
 
-from helpers import network_of
+from helpers import compare_pgm_output, network_of, pgm_output
 from oracle import restate
 
 pytestmark = pytest.mark.gpu
@@ -52,6 +52,13 @@ def test_pgm_json_batch_update_end_to_end(name):
     ref = d["pgm_line"]
     scale_ref = np.max(np.abs(ref), axis=0)
     assert np.all(np.max(np.abs(flows[0] - ref), axis=0) / scale_ref < 1e-7)
+    # the whole PGM output dataset of the input scenario through the writer: node voltages and
+    # injections (device state), line, load and source results
+    _, _, s_bus = b.state()
+    all_flows = branch_flows(net, r.v, base, taps=False, i_n=extra["i_n"])
+    out = pgm.write_output(net, extra, r.v, s_bus, all_flows, base)
+    assert len(out) == len(scale)
+    compare_pgm_output(out[0], pgm_output(d), rtol=1e-7)
     # every scenario against the FP64 oracle on the same S_spec
     for s in range(len(scale)):
         o = restate.nr_solve(net, tol=1e-12, max_iter=40, base_power=base, s_spec=s_spec[s])

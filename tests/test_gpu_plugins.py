@@ -71,6 +71,9 @@ def test_plugins_drop_in_against_reference_backends(name, tmp_path):
     assert abs(ic - ig) <= 1
     if cc:
         assert o["nr_max_dv"][0] < 1e-8 and o["nr_max_dangle"][0] < 1e-8
+    # bus_injections: empty from the reference, S = V conj(Y V) per unit from the plugin
+    n_ref_inj, d_inj, s_inj = o["nr_bus_injections"]
+    assert n_ref_inj == 0 and d_inj <= 1e-12 * max(s_inj, 1.0)
     assert o["mismatch_sizes"][0] == o["mismatch_sizes"][1]
     dm, sm = o["mismatch_max_abs_diff"]
     assert dm <= 1e-9 * sm + 1e-6

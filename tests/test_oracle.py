@@ -157,6 +157,29 @@ def test_pgm_reader_solves_to_power_grid_model(name):
     assert np.array_equal(extra["i_n"], d["pgm_line_i_n"])
 
 
+@pytest.mark.parametrize("name", PGM_JSON)
+def test_pgm_writer_reproduces_power_grid_model_output(name):
+    """pgm.write_output on the oracle's solution (voltages, bus injections, branch results)
+    against power-grid-model's whole output dataset: node, line, sym_load and source results."""
+    from gap_b200 import pgm
+    from helpers import compare_pgm_output, pgm_output
+
+    _, d = network_of(name)
+    net, extra = pgm.read_input(_pgm_json(d))
+    base = float(d["base_power"])
+    r = restate.nr_solve(net, tol=1e-12, max_iter=30, base_power=base)
+    assert r["converged"]
+    rp, ci, va = restate.ybus_reference(net)
+    zb = float(net.u_rated[0]) ** 2 / base
+    s_bus = restate.power_injections(rp, ci, va * zb, r["v"])
+    fl, idx = restate.branch_flows(net, r["v"], base, i_n=extra["i_n"], taps=False)
+    flows = np.zeros((net.n_branch, 9))
+    flows[idx] = fl
+    ours = pgm.write_output(net, extra, r["v"], s_bus, flows, base)
+    worst = compare_pgm_output(ours, pgm_output(d), rtol=1e-9)
+    assert {"node", "line", "sym_load", "source"} <= {c for c, _ in worst}
+
+
 def test_pgm_update_dataset_to_scenarios():
     """A batch update (row and columnar forms) gives per-scenario S_spec with the updated
     loads (as negative injections) and the other appliances unchanged."""
