@@ -157,7 +157,7 @@ __global__ void k_load(PlanDev P, BatchDev B, const double2* __restrict__ y_in,
 // mismatch: fused Y*V SpMV, S = V conj(I), Delta, rhs, per-scenario max |Delta|
 // ---------------------------------------------------------------------------------------
 template <int SW>
-__global__ void __launch_bounds__(256) k_mismatch(PlanDev P, BatchDev B) {
+__global__ void __launch_bounds__(256, 8) k_mismatch(PlanDev P, BatchDev B) {
     const int g = blockIdx.y;
     if (!B.giter[g]) return;
     const int n = P.n_bus;
@@ -1260,7 +1260,7 @@ __global__ void k_solve_bwd(PlanDev P, BatchDev B, double2* out, int accumulate)
 
 // refinement residual: res = rhs - J dx with the FP64 Jacobian blocks
 template <int SW>
-__global__ void __launch_bounds__(256) k_residual(PlanDev P, BatchDev B) {
+__global__ void __launch_bounds__(256, 8) k_residual(PlanDev P, BatchDev B) {
     const int g = blockIdx.y;
     if (!B.gsolve[g] || (B.grefine && !B.grefine[g])) return;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1283,7 +1283,7 @@ __global__ void __launch_bounds__(256) k_residual(PlanDev P, BatchDev B) {
 // voltage update
 // ---------------------------------------------------------------------------------------
 template <int SW>
-__global__ void __launch_bounds__(256) k_update(PlanDev P, BatchDev B) {
+__global__ void __launch_bounds__(256, 8) k_update(PlanDev P, BatchDev B) {
     const int g = blockIdx.y;
     if (!B.gsolve[g]) return;
     const int n = P.n_bus;
