@@ -186,11 +186,11 @@ class Clocks:
 # ------------------------------------------------------------------------------------------
 
 # DRAM bytes per scenario per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
-# ncu --set full capture of the kernel on 320 (dense LU) / 256 (Schur) scenarios of the same
-# grid, scaled by scenarios
+# ncu --set full capture of the kernels on 320 scenarios of the same grid, scaled by scenarios
 # (each scenario's work and bytes are independent of the others).
-MEASURED_TRAFFIC_PER_SCENARIO = {"dense_lu": (1451.35e6 + 1564.00e6) / 320,
-                                 "schur": (83.32e6 + 211.31e6) / 256}
+MEASURED_TRAFFIC_PER_SCENARIO = {"dense_lu": (1451.877e6 + 1568.291e6) / 320,
+                                 "schur": (103.909e6 + 277.920e6) / 320,
+                                 "factor_sparse": (248.066e6 + 205.772e6) / 320}
 
 
 def algorithmic_bytes(kernel, info, n_scen, esz):
@@ -445,7 +445,7 @@ def run_ours(args, rank, world, device):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg,
-                         "traffic_source": "ncu capture on 320 / 256 scenarios, scaled by scenarios"
+                         "traffic_source": "ncu capture on 320 scenarios, scaled by scenarios"
                          if traffic else None,
                          "fp32_fma_tflops": fma_tflops,
                          "launch_ms": kt[dom], "peak_source": "measured" if peaks else "fallback"},
