@@ -65,7 +65,8 @@ class Inputs(C.Structure):
     _fields_ = [("d_y", C.c_void_p), ("d_s_spec", C.c_void_p), ("d_v_init", C.c_void_p),
                 ("d_u_pu", C.c_void_p), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int), ("policy", C.c_int), ("refine", C.c_int),
-                ("refine_below", C.c_double), ("reuse_below", C.c_double)]
+                ("refine_below", C.c_double), ("reuse_below", C.c_double),
+                ("v_init_shared", C.c_int)]
 
 
 class Outputs(C.Structure):

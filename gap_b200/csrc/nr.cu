@@ -226,7 +226,8 @@ void launch_load(gapk_nr_batch b, const gapk_nr_inputs* in, cudaStream_t st) {
     dim3 g(blocks_for((long)P.n_bus * SW, 256), b->G);
     k_load<SW><<<g, 256, 0, st>>>(P, b->dev, reinterpret_cast<const double2*>(in->d_y),
                                   reinterpret_cast<const double2*>(in->d_s_spec),
-                                  reinterpret_cast<const double2*>(in->d_v_init), in->d_u_pu);
+                                  reinterpret_cast<const double2*>(in->d_v_init), in->d_u_pu,
+                                  in->v_init_shared);
 }
 
 template <int SW>
@@ -1282,7 +1283,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
     k_load<1><<<blocks_for((long)n, 256), 256, 0, st>>>(
         P, D, reinterpret_cast<const double2*>(in->d_y),
         reinterpret_cast<const double2*>(in->d_s_spec),
-        reinterpret_cast<const double2*>(in->d_v_init), in->d_u_pu);
+        reinterpret_cast<const double2*>(in->d_v_init), in->d_u_pu, 0);
     rc = check_launch();
     if (rc) return rc;
     const int thr = 512;

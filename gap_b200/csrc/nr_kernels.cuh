@@ -107,7 +107,7 @@ __device__ __forceinline__ void lvl_stamp(BatchDev const& B, int n_levels, int w
 template <int SW>
 __global__ void k_load(PlanDev P, BatchDev B, const double2* __restrict__ y_in,
                        const double2* __restrict__ s_in, const double2* __restrict__ v_in,
-                       const double* __restrict__ u_pu) {
+                       const double* __restrict__ u_pu, int v_shared) {
     const int g = blockIdx.y;
     const int n = P.n_bus;
     const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -119,7 +119,7 @@ __global__ void k_load(PlanDev P, BatchDev B, const double2* __restrict__ y_in,
         B.Sspec[o] = s_in[(size_t)src * n + i];
         double2 v;
         if (v_in) {
-            v = v_in[(size_t)src * n + i];
+            v = v_in[(size_t)(v_shared ? 0 : src) * n + i];
         } else {
             // flat start (cpu_newton_raphson.cpp:77-88): SLACK/PV at u_pu, PQ at 0.98, angle 0
             int t = P.bus_type[i];

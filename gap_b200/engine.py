@@ -235,15 +235,17 @@ class NRBatch:
                 reuse_below=0.0):
         pol = {"reference": N.POLICY_REFERENCE, "newton": N.POLICY_NEWTON,
                "clamped": N.POLICY_CLAMPED}[policy]
+        shared = 1 if v_init is not None and v_init.dim() == 1 else 0
         return N.Inputs(_dptr(y), _dptr(s_spec), _dptr(v_init), _dptr(u_pu), float(tol),
                         int(max_iter), pol, int(refine), float(refine_below),
-                        float(reuse_below))
+                        float(reuse_below), shared)
 
     def solve(self, y, s_spec, v_init=None, u_pu=None, tol=1e-8, max_iter=20,
               policy="reference", refine=0, out=None, stream=None,
               refine_below=0.0, reuse_below=0.0) -> NRResult:
         """y: complex128 per-unit Y values, [nnz] (y_shared) or [S, nnz]; s_spec: complex128
-        [S, n_bus]; v_init: complex128 [S, n_bus] or None (flat start); u_pu: float64
+        [S, n_bus]; v_init: complex128 [S, n_bus], [n_bus] (one start for every scenario) or
+        None (flat start); u_pu: float64
         [n_bus] flat-start |V| of SLACK/PV buses.  refine_below > 0 runs the `refine`
         refinement steps only in iterations where a scenario of the lane group has max
         |mismatch| below it.  reuse_below > 0 keeps a group's previous LU factors once all
@@ -428,9 +430,11 @@ class HostPipeline:
 
     def solve(self, y, s_host, v_host, out_v, out_status=None, out_iterations=None,
               out_mismatch=None, **kw):
-        """y: device per-unit Y [nnz]; s_host, v_host: host complex128 [S, n_bus]; results
-        into the host tensors out_v [S, n_bus] (and optionally status, iterations, final
-        mismatch [S]).  Returns after every part's results are on the host."""
+        """y: device per-unit Y [nnz]; s_host: host complex128 [S, n_bus]; v_host: host
+        complex128 [S, n_bus], or [n_bus] for one start vector shared by every scenario (copied
+        once per part); results into the host tensors out_v [S, n_bus] (and optionally status,
+        iterations, final mismatch [S]).  Returns after every part's results are on the
+        host."""
         torch = _torch()
         cur = torch.cuda.current_stream()
         for st in self.streams:
@@ -438,7 +442,7 @@ class HostPipeline:
         for (a, b), bt, st in zip(self.ranges, self.batches, self.streams):
             with torch.cuda.stream(st):
                 sd = s_host[a:b].to("cuda", non_blocking=True)
-                vd = v_host[a:b].to("cuda", non_blocking=True)
+                vd = (v_host if v_host.dim() == 1 else v_host[a:b]).to("cuda", non_blocking=True)
                 r = bt.solve(y, sd, v_init=vd, stream=st, **kw)
                 out_v[a:b].copy_(r.v, non_blocking=True)
                 for host, dev in ((out_status, r.status), (out_iterations, r.iterations),

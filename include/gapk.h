@@ -215,6 +215,7 @@ typedef struct {
                                below this, the group keeps its previous LU factors instead of
                                refactorising, and the (refined, refine >= 1) solve uses them
                                against the current FP64 Jacobian (0 = refactorise every time) */
+    int v_init_shared;      /* != 0: d_v_init is one start vector [n_bus] for every scenario */
 } gapk_nr_inputs;
 
 typedef struct {

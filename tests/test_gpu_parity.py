@@ -587,6 +587,15 @@ def test_host_pipeline_equals_one_batch():
         assert torch.equal(vo, one.v.cpu())
         assert torch.equal(st, one.status.cpu()) and (st.numpy() == 0).all()
         assert torch.equal(it, one.iterations.cpu())
+    # one start vector shared by every scenario (v_init_shared): the same results, from the
+    # pipeline and from a device batch
+    v_h1 = torch.as_tensor(v0[0]).pin_memory()
+    pipe.solve(y, s_h, v_h1, vo, st, it, **kw)
+    assert torch.equal(vo, one.v.cpu()) and torch.equal(it, one.iterations.cpu())
+    shared = NRBatch(plan, S, precision="fp32", lanes=8, threads=1024).solve(
+        y, torch.as_tensor(s_spec, device="cuda"), v_init=torch.as_tensor(v0[0], device="cuda"),
+        **kw)
+    assert torch.equal(shared.v, one.v) and torch.equal(shared.iterations, one.iterations)
 
 
 def test_factor_reuse_near_convergence_matches_oracle():
