@@ -151,6 +151,7 @@ struct gapk_nr_plan_s {
 struct gapk_nr_batch_s {
     gapk_nr_plan plan = nullptr;
     int n_scen = 0, sw = 8, G = 0, precision = 0, y_shared = 1, threads = 256, use_graph = 1;
+    int dense_fused = 0;
     DevBuf V, Sspec, Scalc, Y, F, A64, rhs, dx, res, X, Dt, mis, state, solving, singular,
         iters, status, fmis, gsolve, giter, grefine, gfactor, ctrl, tol;
     int dense_w = 0;          // panel width of the one-CTA-per-scenario dense LU (0: not used)
@@ -642,6 +643,7 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     }
     b->threads = thr;
     b->use_graph = opt ? opt->use_graph : 1;
+    b->dense_fused = opt ? opt->dense_fused : 0;
     int rc = p->upload();
     if (rc) return rc;
     auto const& h = p->h;
@@ -682,7 +684,7 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
         int dev = 0, n_sm = 148;
         if (cudaGetDevice(&dev) == cudaSuccess)
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-        b->dense_split = b->dense_w == 0 || L < 2 * (size_t)n_sm;
+        b->dense_split = b->dense_w == 0 || (L < 2 * (size_t)n_sm && !b->dense_fused);
         A(b->Dt, L * N * dense_ld((int)N) * esz);
         if (!b->dense_split) {
             cudaError_t e = b->precision == GAPK_PREC_FP64

@@ -213,7 +213,7 @@ class NRBatch:
     """Device state for n_scen scenarios sharing one NRPlan."""
 
     def __init__(self, plan: NRPlan, n_scen: int, precision="fp64", y_shared=True, lanes=0,
-                 threads=0, use_graph=True):
+                 threads=0, use_graph=True, dense_fused=False):
         require_cuda()
         self.plan = plan
         self.n_scen = int(n_scen)
@@ -221,7 +221,7 @@ class NRBatch:
         self.y_shared = bool(y_shared)
         opt = N.BatchOptions(N.PREC_FP64 if precision == "fp64" else N.PREC_FP32,
                              1 if y_shared else 0, int(lanes), int(threads),
-                             1 if use_graph else 0)
+                             1 if use_graph else 0, 1 if dense_fused else 0)
         h = C.c_void_p()
         N.check(N.lib().gapk_nr_batch_create(plan._h, C.c_int(self.n_scen), C.byref(opt),
                                              C.byref(h)))
@@ -422,7 +422,10 @@ class HostPipeline:
         step = -(-n_scen // chunks)
         step = -(-step // max(1, lanes)) * max(1, lanes)
         self.ranges = [(a, min(a + step, n_scen)) for a in range(0, n_scen, step)]
-        self.batches = [NRBatch(plan, b - a, precision=precision, lanes=lanes, threads=threads)
+        # the parts run concurrently and together fill the GPU: each keeps the
+        # one-CTA-per-scenario dense LU even when it alone would not
+        self.batches = [NRBatch(plan, b - a, precision=precision, lanes=lanes, threads=threads,
+                                dense_fused=len(self.ranges) > 1)
                         for a, b in self.ranges]
         self.streams = [torch.cuda.Stream() for _ in self.ranges]
         self.plan = plan

@@ -184,6 +184,9 @@ typedef struct {
     int lanes;          /* scenarios interleaved per thread group: 1, 2, 4 or 8 (0 = auto) */
     int threads;        /* threads per CTA of the factor / solve kernels (0 = auto)        */
     int use_graph;      /* 1: NR loop as a CUDA graph with a device-side while node        */
+    int dense_fused;    /* 1: one-CTA-per-scenario dense-tail LU even for a batch too small
+                           to fill the GPU alone (batches that run concurrently on several
+                           streams); 0: chosen by the batch size                           */
 } gapk_nr_batch_options;
 
 int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options* opt,

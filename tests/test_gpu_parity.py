@@ -546,6 +546,13 @@ def test_dense_tail_paths_agree():
     assert (rb.status.cpu().numpy() == 0).all() and (rs.status.cpu().numpy() == 0).all()
     Vb, Vs = rb.v.cpu().numpy(), rs.v.cpu().numpy()
     assert np.max(np.abs(Vb[:8] - Vs)) < 1e-9
+    # dense_fused: the small batch on the one-CTA-per-scenario kernel (as the parts of a
+    # HostPipeline run) gives the large batch's voltages
+    fused = NRBatch(plan, 8, precision="fp32", lanes=8, dense_fused=True)
+    rf = fused.solve(y, torch.as_tensor(s_spec[:8], device="cuda"),
+                     v_init=torch.as_tensor(v0[:8], device="cuda"), **kw)
+    assert (rf.status.cpu().numpy() == 0).all()
+    assert np.max(np.abs(rf.v.cpu().numpy() - Vb[:8])) < 1e-12
     Y = restate.ybus_pi(net)
     for s in (0, 299):
         o = restate.nr_solve(net, Y=Y, tol=1e-12, max_iter=30, base_power=base,
@@ -572,7 +579,9 @@ def test_host_pipeline_equals_one_batch():
                     torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
     plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
     kw = dict(tol=1e-10, max_iter=30, policy="newton", refine=1, refine_below=1e-4)
-    one = NRBatch(plan, S, precision="fp32", lanes=8, threads=1024).solve(
+    # the pipeline's parts use the one-CTA-per-scenario dense LU (dense_fused); so does the
+    # reference batch here
+    one = NRBatch(plan, S, precision="fp32", lanes=8, threads=1024, dense_fused=True).solve(
         y, torch.as_tensor(s_spec, device="cuda"), v_init=torch.as_tensor(v0, device="cuda"),
         **kw)
     s_h = torch.as_tensor(s_spec).pin_memory()
@@ -592,7 +601,7 @@ def test_host_pipeline_equals_one_batch():
     v_h1 = torch.as_tensor(v0[0]).pin_memory()
     pipe.solve(y, s_h, v_h1, vo, st, it, **kw)
     assert torch.equal(vo, one.v.cpu()) and torch.equal(it, one.iterations.cpu())
-    shared = NRBatch(plan, S, precision="fp32", lanes=8, threads=1024).solve(
+    shared = NRBatch(plan, S, precision="fp32", lanes=8, threads=1024, dense_fused=True).solve(
         y, torch.as_tensor(s_spec, device="cuda"), v_init=torch.as_tensor(v0[0], device="cuda"),
         **kw)
     assert torch.equal(shared.v, one.v) and torch.equal(shared.iterations, one.iterations)
