@@ -71,3 +71,64 @@ def compare_pgm_output(ours, ref, rtol):
     bad = {k: w for k, w in worst.items() if not w < rtol}
     assert not bad, bad
     return worst
+
+
+def random_network(seed, n_max=40):
+    """A seeded random small network for fuzzing the device path against the oracle: a random
+    tree plus extra branches (parallel duplicates and an out-of-service one among them), 10 kV
+    per-unit-like impedances, a few transformers with taps / phase shifts, shunts, PV buses
+    (about 20%), one slack (bus 0), light loads and generation, bus IDs shuffled."""
+    from gap_b200.network import LOADGEN, PQ, PV, SHUNT, SLACK, Network
+
+    rng = np.random.default_rng(1000 + seed)
+    n = int(rng.integers(3, n_max + 1))
+    ids = rng.permutation(np.arange(10, 10 + 3 * n, 3))[:n]
+    frm, to = [], []
+    for i in range(1, n):
+        frm.append(int(rng.integers(0, i)))
+        to.append(i)
+    for _ in range(int(rng.integers(0, max(2, n // 3)))):
+        a, b = (int(x) for x in rng.choice(n, 2, replace=False))
+        frm.append(a)
+        to.append(b)
+    if len(frm) > 2 and rng.random() < 0.5:  # a parallel duplicate of an existing branch
+        j = int(rng.integers(0, len(frm)))
+        frm.append(frm[j])
+        to.append(to[j])
+    m = len(frm)
+    zb = 10e3 ** 2 / 1e6
+    x = rng.uniform(0.02, 0.12, m) * zb
+    r = x * rng.uniform(0.1, 0.5, m)
+    b = rng.uniform(0.0, 0.02, m) / zb
+    k = np.ones(m)
+    th = np.zeros(m)
+    tr = rng.random(m) < 0.15
+    k[tr] = rng.uniform(0.95, 1.05, tr.sum())
+    th[tr] = rng.uniform(0.0, 0.1, tr.sum())
+    status = np.ones(m, np.int32)
+    if m > n:  # an extra branch out of service (the tree stays connected)
+        status[int(rng.integers(n - 1, m))] = 0
+    bt = np.full(n, PQ, np.int32)
+    bt[0] = SLACK
+    pv = rng.random(n) < 0.2
+    pv[0] = False
+    bt[pv] = PV
+    u_pu = np.ones(n)
+    u_pu[0] = rng.uniform(1.0, 1.05)
+    u_pu[pv] = rng.uniform(0.99, 1.04, pv.sum())
+    p = np.zeros(n)
+    q = np.zeros(n)
+    load = rng.uniform(0.0, 0.25e6, n)
+    p[1:] = -load[1:]
+    q[1:] = -load[1:] * rng.uniform(0.1, 0.4, n - 1)
+    p[pv] = rng.uniform(0.05e6, 0.3e6, pv.sum())
+    app_node, app_type, app_g1, app_b1 = [], [], [], []
+    for i in np.nonzero(rng.random(n) < 0.15)[0]:
+        app_node.append(int(ids[i]))
+        app_type.append(SHUNT)
+        app_g1.append(0.0)
+        app_b1.append(float(rng.uniform(-0.02, 0.02) / zb))
+    return Network.build(bus_id=ids, u_rated=np.full(n, 10e3), bus_type=bt, u_pu=u_pu, p=p, q=q,
+                         from_id=ids[frm], to_id=ids[to], r1=r, x1=x, b1=b, k=k, theta=th,
+                         status=status, app_node=app_node, app_type=app_type, app_g1=app_g1,
+                         app_b1=app_b1)
