@@ -9,6 +9,16 @@ namespace gapk {
 
 void set_error(std::string const& msg);
 
+// NVTX range over a host call (plan analysis, batch set-up, solve enqueue, stages), so that a
+// profiler's timeline names the engine's phases; without a tool attached a push/pop costs a few
+// nanoseconds.  Defined in nr.cu (NVTX v3, header only).
+struct TraceRange {
+    explicit TraceRange(const char* name);
+    ~TraceRange();
+    TraceRange(TraceRange const&) = delete;
+    TraceRange& operator=(TraceRange const&) = delete;
+};
+
 // ---- Y-bus pattern -------------------------------------------------------------------
 // Source encoding of one CSR slot:
 //   off-diagonal triplet of branch b in direction d (0: (from,to), 1: (to,from)) -> 2*b + d

@@ -9,6 +9,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/gapk.h"
 #include "internal.h"
 #include "nr_kernels.cuh"
@@ -511,6 +513,7 @@ int gapk_device_count(void) {
 int gapk_nr_plan_create(int n_bus, int nnz_y, const int* h_y_row_ptr, const int* h_y_col_idx,
                         const int* h_bus_type, const gapk_nr_plan_options* opt,
                         gapk_nr_plan* out) {
+    TraceRange tr("gapk_nr_plan_create: ordering and symbolic analysis");
     if (!out || n_bus < 0 || nnz_y < 0 || !h_y_row_ptr || (nnz_y && !h_y_col_idx) ||
         (n_bus && !h_bus_type)) {
         set_error("gapk_nr_plan_create: bad arguments");
@@ -615,6 +618,7 @@ int64_t gapk_nr_plan_export(gapk_nr_plan p, int what, int* h_buf) {
 
 int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options* opt,
                          gapk_nr_batch* out) {
+    TraceRange tr("gapk_nr_batch_create");
     if (!p || !out || n_scen <= 0) {
         set_error("gapk_nr_batch_create: bad arguments");
         return GAPK_EINVAL;
@@ -766,6 +770,7 @@ int64_t gapk_nr_batch_device_bytes(gapk_nr_batch b) {
 
 int gapk_nr_solve(gapk_nr_batch b, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
                   void* stream) {
+    TraceRange tr("gapk_nr_solve");
     if (!b) {
         set_error("gapk_nr_solve: null batch");
         return GAPK_EINVAL;
@@ -820,6 +825,9 @@ static int stage(gapk_nr_batch b, int which, void* stream) {
         set_error("stage: null batch");
         return GAPK_EINVAL;
     }
+    static const char* names[] = {"gapk stage: mismatch", "gapk stage: jacobian",
+                                  "gapk stage: factor", "gapk stage: solve", "gapk stage: update"};
+    TraceRange tr(which >= 0 && which < 5 ? names[which] : "gapk stage");
     dispatch_tsw<StageOp>(b->precision, b->sw, b, which, static_cast<cudaStream_t>(stream));
     return check_launch();
 }
@@ -877,6 +885,7 @@ int gapk_nr_stage_get_mismatch(gapk_nr_batch b, double* d_f, void* stream) {
 }
 
 int gapk_nr_step(gapk_nr_batch b, int* h_active, void* stream) {
+    TraceRange tr("gapk_nr_step: one Newton iteration");
     if (!b || !h_active) {
         set_error("gapk_nr_step: bad arguments");
         return GAPK_EINVAL;
@@ -1319,3 +1328,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
     }
     return GAPK_OK;
 }
+
+// NVTX range helper of internal.h
+gapk::TraceRange::TraceRange(const char* name) { nvtxRangePushA(name); }
+gapk::TraceRange::~TraceRange() { nvtxRangePop(); }

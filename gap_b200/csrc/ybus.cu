@@ -235,6 +235,7 @@ extern "C" {
 int gapk_ybus_create(int n_bus, int n_branch, const int* h_from_idx, const int* h_to_idx,
                      const int* h_in_service, int n_shunt, const int* h_shunt_bus,
                      gapk_ybus* out) {
+    TraceRange tr("gapk_ybus_create: Y-bus pattern");
     if (!out || n_bus < 0 || n_branch < 0 || n_shunt < 0 ||
         (n_branch && (!h_from_idx || !h_to_idx || !h_in_service)) || (n_shunt && !h_shunt_bus)) {
         set_error("gapk_ybus_create: bad arguments");
@@ -267,6 +268,7 @@ int gapk_ybus_pattern(gapk_ybus y, int* h_row_ptr, int* h_col_idx) {
 int gapk_ybus_assemble(gapk_ybus y, int n_scen, const double* d_branch, int64_t branch_stride,
                        const double* d_shunt, int64_t shunt_stride, int mode, double scale,
                        double* d_values, int64_t values_stride, void* stream) {
+    TraceRange tr("gapk_ybus_assemble");
     if (!y || n_scen <= 0 || !d_values || (y->h.n_branch && !d_branch) ||
         (y->h.n_shunt && !d_shunt) || (mode != GAPK_YBUS_REFERENCE && mode != GAPK_YBUS_TAPS) ||
         branch_stride < 0 || shunt_stride < 0 || (n_scen > 1 && values_stride < y->h.nnz)) {
