@@ -251,3 +251,37 @@ def test_contingency_params_equal_branch_outage():
         keep[e] = False
         g = sp.coo_matrix((np.ones(keep.sum()), (f[keep], t[keep])), shape=(net.n_bus,) * 2)
         assert connected_components(g, directed=False)[0] > 1
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """The Python binding's ctypes structures have the C header's layout: every field at the
+    offset and every struct of the size that a C compiler gives include/gapk.h."""
+    import ctypes as C
+    import shutil
+    import subprocess
+
+    from gap_b200 import _native as N
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"gapk_nr_plan_options": N.PlanOptions, "gapk_nr_plan_info": N.PlanInfo,
+               "gapk_nr_batch_options": N.BatchOptions, "gapk_nr_inputs": N.Inputs,
+               "gapk_nr_outputs": N.Outputs}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "gapk.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = {tuple(line.split()[:2]): int(line.split()[2]) for line in out.splitlines()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
