@@ -288,6 +288,38 @@ bool analyze_nr(int n_bus, int nnz_y, const int* y_row_ptr, const int* y_col_idx
         std::vector<int> fp(P.level_ptr.begin(), P.level_ptr.end() - 1);
         for (int k = 0; k < ns; ++k) P.level_nodes[fp[height[k]]++] = k;
     }
+    // Renumber the sparse nodes level by level (stable within a level).  Children have lower
+    // heights than their parents, so this is another topological order of the same elimination
+    // tree: the same fill, the same parents (a column's first entry), with the nodes of one
+    // level contiguous, so that the level-scheduled kernels read their right-hand sides,
+    // solutions, pivots and column pointers as contiguous runs.  The tail keeps its numbers.
+    if (ns > 0) {
+        std::vector<int> newk(nb);
+        for (int t = 0; t < ns; ++t) newk[P.level_nodes[t]] = t;
+        for (int k = ns; k < nb; ++k) newk[k] = k;
+        std::vector<int> bus_of_node(nb), node_pq(nb), lptr(nb + 1, 0), lidx(P.nnz_l), lev(ns);
+        for (int k = 0; k < nb; ++k) {
+            const int k2 = newk[k];
+            bus_of_node[k2] = P.bus_of_node[k];
+            node_pq[k2] = P.node_pq[k];
+            lptr[k2 + 1] = P.lptr[k + 1] - P.lptr[k];
+        }
+        for (int k = 0; k < nb; ++k) lptr[k + 1] += lptr[k];
+        for (int k = 0; k < nb; ++k) {
+            const int k2 = newk[k];
+            int w = lptr[k2];
+            for (int p = P.lptr[k]; p < P.lptr[k + 1]; ++p) lidx[w++] = newk[P.lidx[p]];
+            std::sort(lidx.begin() + lptr[k2], lidx.begin() + lptr[k2 + 1]);
+        }
+        for (int k = 0; k < ns; ++k) lev[newk[k]] = height[k];
+        P.bus_of_node.swap(bus_of_node);
+        P.node_pq.swap(node_pq);
+        P.lptr.swap(lptr);
+        P.lidx.swap(lidx);
+        P.node_level.swap(lev);
+        for (int k = 0; k < nb; ++k) P.node_of_bus[P.bus_of_node[k]] = k;
+        for (int t = 0; t < ns; ++t) P.level_nodes[t] = t;
+    }
 
     // Y sources per (row bus, col bus): rows of (col, index), sorted by col then index
     std::vector<std::pair<int, int>> yrow;
