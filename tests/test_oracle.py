@@ -203,3 +203,66 @@ def test_pgm_update_dataset_to_scenarios():
         for i, f in enumerate(scale):
             assert np.allclose(s[i].real, f * s0.real, rtol=1e-12, atol=0)
             assert np.allclose(s[i].imag, s0.imag, rtol=1e-12, atol=0)
+
+
+def test_pgm_writer_components_and_balances():
+    """pgm.write_output on a PGM input with every component kind the reader takes (line,
+    transformer, generic_branch, source, sym_load, sym_gen, shunt): each result lands under its
+    component, node injections equal the node's appliances (source + generation - load), and
+    the branch results at each end sum to the node injections less the shunts' power."""
+    from gap_b200 import pgm
+
+    doc = {"data": {
+        "node": [{"id": 1, "u_rated": 10500.0}, {"id": 2, "u_rated": 10500.0},
+                 {"id": 3, "u_rated": 10500.0}, {"id": 4, "u_rated": 10500.0}],
+        "line": [{"id": 10, "from_node": 1, "to_node": 2, "from_status": 1, "to_status": 1,
+                  "r1": 0.3, "x1": 0.4, "c1": 1e-7, "tan1": 0.0, "i_n": 500.0}],
+        "transformer": [{"id": 11, "from_node": 2, "to_node": 3, "from_status": 1,
+                         "to_status": 1, "u1": 10500.0, "u2": 10500.0, "sn": 2e6, "uk": 0.06,
+                         "pk": 2e4, "i0": 0.0, "p0": 0.0, "rx_ratio": 0.1}],
+        "generic_branch": [{"id": 12, "from_node": 3, "to_node": 4, "from_status": 1,
+                            "to_status": 1, "r1": 0.2, "x1": 0.5, "g1": 0.0, "b1": 0.0,
+                            "k": 1.0, "shift": 0.0, "sn": 1e6}],
+        "source": [{"id": 20, "node": 1, "status": 1, "u_ref": 1.02}],
+        "sym_load": [{"id": 30, "node": 3, "status": 1, "type": 0, "p_specified": 4e5,
+                      "q_specified": 1e5}, {"id": 31, "node": 4, "status": 1, "type": 0,
+                                            "p_specified": 3e5, "q_specified": 5e4}],
+        "sym_gen": [{"id": 40, "node": 2, "status": 1, "type": 0, "p_specified": 1e5,
+                     "q_specified": 0.0}],
+        "shunt": [{"id": 50, "node": 4, "status": 1, "g1": 0.0, "b1": 1e-4}],
+    }}
+    net, extra = pgm.read_input(doc)
+    base = 1e6
+    r = restate.nr_solve(net, tol=1e-12, max_iter=30, base_power=base, policy="newton",
+                         Y=restate.ybus_pi(net), jac="exact")
+    assert r["converged"]
+    rp, ci, va = restate.ybus_pi(net)
+    zb = float(net.u_rated[0]) ** 2 / base
+    s_bus = restate.power_injections(rp, ci, va * zb, r["v"])
+    fl, idx = restate.branch_flows(net, r["v"], base, i_n=extra["i_n"], sn=extra["sn"])
+    flows = np.zeros((net.n_branch, 9))
+    flows[idx] = fl
+    out = pgm.write_output(net, extra, r["v"], s_bus, flows, base)
+    assert {c: len(v) for c, v in out.items()} == {"node": 4, "line": 1, "transformer": 1,
+                                                   "generic_branch": 1, "source": 1,
+                                                   "sym_load": 2, "sym_gen": 1}
+    node = {n["id"]: n for n in out["node"]}
+    src = out["source"][0]
+    assert src["p"] == pytest.approx(node[1]["p"], rel=1e-12)
+    assert node[2]["p"] == pytest.approx(1e5, rel=1e-9)
+    assert node[3]["p"] == pytest.approx(-4e5, rel=1e-9)
+    assert node[4]["q"] == pytest.approx(-5e4, rel=1e-9)
+    assert out["sym_load"][0]["p"] == 4e5 and out["sym_gen"][0]["p"] == 1e5
+    assert src["i"] == pytest.approx(np.hypot(src["p"], src["q"]) /
+                                     (np.sqrt(3) * node[1]["u"]), rel=1e-12)
+    # every node's injection flows out through its branch ends (the shunt's power is inside
+    # the node injection's Y V), so with the shunt at bus 4 its reactive balance closes on Y
+    ends = {1: [("line", "from")], 2: [("line", "to"), ("transformer", "from")],
+            3: [("transformer", "to"), ("generic_branch", "from")],
+            4: [("generic_branch", "to")]}
+    for nid, lst in ends.items():
+        p_out = sum(out[c][0]["p_" + e] for c, e in lst)
+        assert p_out == pytest.approx(node[nid]["p"], rel=1e-9, abs=1e-3)
+    gb = out["generic_branch"][0]
+    assert gb["loading"] == pytest.approx(max(gb["i_from"], gb["i_to"]) / extra["i_n"][2],
+                                          rel=1e-12)
