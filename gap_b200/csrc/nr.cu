@@ -671,9 +671,10 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     A(b->X, L * nb * 2 * esz);
     if (h.n_tail > 0) {
         // Dense-tail LU: one CTA per scenario (k_dense_lu, the panel in shared memory) when
-        // there are enough scenarios to fill the GPU and the panel fits; otherwise the split
-        // kernels, which spread each scenario's trailing update over many CTAs and have no
-        // shared-memory limit on the tail size.
+        // there are enough scenarios to fill the GPU (or the caller says that concurrent
+        // batches will, dense_fused) and the panel fits; otherwise the split kernels, which
+        // spread each scenario's trailing update over many CTAs and have no shared-memory
+        // limit on the tail size.
         const size_t N = 2 * (size_t)h.n_tail;
         const size_t smem_max = 232448 - 1024;  // opt-in shared memory per block, less static
         b->dense_w = 0;
