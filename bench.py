@@ -23,7 +23,7 @@ Supplementary workloads (one GPU, not the headline):
          and 64 independent grids with n log-uniform in [500, 20000], all solved concurrently
          (one CUDA stream and graph per study, lanes/threads autotuned per study).
   large  32 load scenarios of a 100k-bus grid of the same generator (accuracy against the
-         FP64 oracle: tests/test_gpu_large.py, run with GAP_B200_LARGE=1).
+         FP64 oracle: tests/test_gpu_large.py).
 """
 
 from __future__ import annotations
@@ -42,29 +42,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Power-flow solves/s on 1 B200: batched mixed-precision vs plain FP64 at 1e-8 pu"
-N_BUS = 10_000
-GRID_SEED = 0
-N_SCEN = 1024
-SIGMA = 0.1
-TOL = 1e-8
-MAX_ITER = 20
-BASE = 1e8
-# FP64 refinement steps per Newton correction once a lane group's max |mismatch| < 1e-2 pu
-REFINE_STEPS = 2
-REFINE_BELOW = 1e-2
-# ... and below the same mismatch the lane group keeps its previous LU factors
-REUSE_BELOW = 1e-2
+from gap_b200.workloads import (BASE, GRID_SEED, MAX_ITER, N_BUS, REFINE_BELOW,  # noqa: E402
+                                REFINE_STEPS, REUSE_BELOW, SIGMA, TOL)
+from gap_b200 import workloads  # noqa: E402
+
+N_SCEN = workloads.N_SCEN
 # per-bus load scale of the large (100k-bus) workload
 LARGE_LOAD_SCALE = 0.025
 
 
 def workload(rank: int):
-    from gap_b200 import synth
-
-    net = synth.transmission_grid(GRID_SEED, n=N_BUS)
-    s_spec = synth.load_scenarios(net, N_SCEN, sigma=SIGMA, seed=1 + rank, base_power=BASE)
-    # one start (DC angles) shared by every scenario
-    return net, s_spec, synth.dc_start(net, BASE)
+    return workloads.headline(rank, N_SCEN)
 
 
 def config(extra=None):
@@ -73,7 +61,8 @@ def config(extra=None):
          "max_iter": MAX_ITER,
          "precision": "fp32 factor+solve, fp64 mismatch/update; below 1e-2 pu: 2 refinement "
                       "steps, factors reused",
-         "policy": "newton", "start": "dc angles", "l2": "inputs larger than L2 (state > 300 MB)"}
+         "policy": "newton", "start": "dc angles", "l2": "inputs larger than L2 (state > 300 MB)",
+         "generator_deviations": dict(workloads.DEVIATIONS)}
     if extra:
         c.update(extra)
     return c
@@ -269,15 +258,12 @@ def run_ours(args, rank, world, device):
     plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
     plan_s = time.perf_counter() - t0
     info = plan.info
-    batch = NRBatch(plan, N_SCEN, precision="fp32", lanes=8, threads=1024,
-                    use_graph=not args.host_loop)
+    batch = NRBatch(plan, N_SCEN, use_graph=not args.host_loop, **workloads.batch_kwargs())
     s_dev = torch.as_tensor(s_np, device="cuda")
     v_dev = torch.as_tensor(v_np, device="cuda")
 
     def step():
-        return batch.solve(y, s_dev, v_init=v_dev, tol=TOL, max_iter=MAX_ITER, policy="newton",
-                           refine=REFINE_STEPS, refine_below=REFINE_BELOW,
-                           reuse_below=REUSE_BELOW)
+        return batch.solve(y, s_dev, v_init=v_dev, **workloads.solve_kwargs())
 
     for _ in range(args.warmup):
         r = step()
@@ -310,12 +296,10 @@ def run_ours(args, rank, world, device):
 
     # four parts on four streams: one part's copies overlap the other parts' solves (each part
     # keeps the one-CTA-per-scenario dense LU, dense_fused)
-    pipe = HostPipeline(plan, N_SCEN, chunks=4, precision="fp32", lanes=8, threads=1024)
+    pipe = HostPipeline(plan, N_SCEN, chunks=4, **workloads.batch_kwargs())
 
     def e2e_step():
-        pipe.solve(y, s_h, v_h, vo_h, st_h, it_h, fm_h, tol=TOL, max_iter=MAX_ITER,
-                   policy="newton", refine=REFINE_STEPS, refine_below=REFINE_BELOW,
-                   reuse_below=REUSE_BELOW)
+        pipe.solve(y, s_h, v_h, vo_h, st_h, it_h, fm_h, **workloads.solve_kwargs())
 
     e2e_step()
     torch.cuda.synchronize()

@@ -1112,12 +1112,12 @@ int gapk_splu_size(gapk_splu s) { return s ? s->plan.h.nb : GAPK_EINVAL; }
 // ===========================================================================================
 // Allocation-free single-scenario solve.
 //
-// Some callers cannot call cudaMalloc at solve time: code that runs while another library
-// holds the device in stream capture, hosts that hand out device memory only from their own
-// pools, and real-time loops that must not touch the allocator.  gapk_nr_solve_noalloc serves
-// them: it solves one scenario in FP64 with the same kernels as gapk_nr_solve, but every
-// buffer it needs (a copy of the plan's index lists and the whole Newton state) is carved out
-// of one file-scope device array of fixed size.  The caller passes only inputs and outputs.
+// Some callers cannot call cudaMalloc at solve time: hosts that hand out device memory only
+// from their own pools, and real-time loops that must not touch the allocator (cudaMalloc and
+// cudaFree can block on the whole device).  gapk_nr_solve_noalloc serves them: it solves one
+// scenario in FP64 with the same kernels as gapk_nr_solve, but every buffer it needs (a copy
+// of the plan's index lists and the whole Newton state) is carved out of one file-scope device
+// array of fixed size.  The caller passes only inputs and outputs.
 // ===========================================================================================
 namespace {
 
@@ -1202,9 +1202,10 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
     size_t dense_smem = 0;
     int dense_w = 0;
     if (h.n_tail > 0) {
+        // the panel width rule of gapk_nr_batch_create for FP64 tails
         for (int w : {32, 16, 8}) {
             size_t bytes = dense_lu_elems((int)N, w) * 8;
-            if (bytes <= 232448 - 1024) {
+            if (bytes <= 232448 - 1024 && (w < 32 || N <= 200)) {
                 dense_w = w;
                 dense_smem = bytes;
                 break;
@@ -1327,6 +1328,9 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
         rc = check_launch();
         if (rc) return rc;
     }
+    // the outputs are read from the shared scratch: wait for them, so that a later call from
+    // this thread (on any stream) cannot overwrite the scratch before they are written
+    GAPK_CUDA_TRY(cudaStreamSynchronize(st));
     return GAPK_OK;
 }
 

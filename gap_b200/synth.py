@@ -62,9 +62,10 @@ def feeder_grid(seed: int = 0, n: int = 200, tie_frac: float = 0.10) -> Network:
 TRANSMISSION_KV = 138.0
 BASE_MVA = 100.0
 # Per-bus loads are p ~ U[0,1] * LOAD_SCALE pu.  With LOAD_SCALE = 1 (0-100 MW at every bus of
-# a 100 MVA-base grid with x ~ U[0.01,0.2]) no power-flow solution exists at 10k buses (the
-# FP64 Newton iteration collapses the voltages), and at 0.1 about 2 % of the lognormal load
-# scenarios of the 10k-bus grid have none; 0.05 leaves every scenario solvable.
+# a 100 MVA-base grid with x ~ U[0.01,0.2]) no power-flow solution exists at 10k buses: a
+# load-scale continuation of the 10k-bus base case ends at its nose point near 0.23
+# (tests/test_workload_loading.py), and lognormal scenarios (sigma 0.1) around 0.2 already
+# fail; 0.05 leaves every scenario solvable.
 LOAD_SCALE = 0.05
 
 

@@ -302,19 +302,23 @@ int gapk_splu_factorize(gapk_splu s, const double* d_values, void* stream);
 int gapk_splu_solve(gapk_splu s, const double* d_rhs, double* d_x, void* stream);
 
 /* Allocation-free variant of gapk_nr_solve for ONE scenario in FP64 (no counterpart in the
- * reference).  For callers that may not allocate device memory while they solve -- code
- * running inside another library's stream capture, hosts that own all device memory through
- * their own pools, real-time loops that must not touch the allocator.  It calls no cudaMalloc,
- * cudaFree or allocating library routine: the plan's index lists are copied into, and the
- * whole Newton state lives in, one static 32 MiB device array that every GPU loading the
- * library holds until the process exits.  Grids whose plan and state need more than 32 MiB
- * (roughly beyond 10k buses) are rejected with GAPK_ERANGE.  `in` as for gapk_nr_solve with
- * refine = 0 (d_y shared, d_s_spec / d_v_init / outputs for one scenario); the loop is
- * host-driven (one stream synchronisation per iteration).  The first call on a device looks
- * up the array's device address and sets a kernel attribute; make that first call before
- * any stream capture.  All calls share the one array, so calls that overlap on the GPU (from
- * several host threads or streams) race and corrupt each other; the array keeps the last
- * call's contents, and every call reinitialises what it reads. */
+ * reference).  For callers that may not allocate device memory while they solve: hosts that
+ * own all device memory through their own pools and hand none to plugins, and real-time
+ * loops that must not call into the allocator (cudaMalloc / cudaFree can block on the whole
+ * device).  It calls no cudaMalloc, cudaFree or allocating library routine: the plan's index
+ * lists are copied into, and the whole Newton state lives in, one static 32 MiB device array
+ * that every GPU loading the library holds until the process exits.  Grids whose plan and
+ * state need more than 32 MiB (beyond about 15k buses of the transmission-like generator;
+ * 10k-bus grids fit) are rejected with GAPK_ERANGE.  `in` as for gapk_nr_solve with
+ * refine = 0 (d_y shared, d_s_spec / d_v_init / outputs for one scenario).  The loop is driven
+ * from the host: the call copies the plan's index lists from host memory, waits for `stream`
+ * once per Newton iteration and once more after writing the outputs, so the outputs are ready
+ * when it returns; pass a stream created with cudaStreamNonBlocking so that these waits do
+ * not also wait for work on the legacy default stream.  The first call on a device looks up
+ * the array's device address and sets a kernel attribute; make that first call before any
+ * stream capture.  All calls share the one array, so calls that overlap on the GPU (from
+ * several host threads at once) race and corrupt each other; the array keeps the last call's
+ * contents, and every call reinitialises what it reads. */
 int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
                           void* stream);
 

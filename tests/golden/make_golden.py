@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference project next to it (default /root/reference) and
+Run in a checkout that has the reference project next to it and
 the reference oracle built (make -C oracle):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <path of the reference checkout>
 
 Fixtures (all small .npz files):
   pgm_<case>.npz   the reference's PGM validation cases (tests/pgm_validation/test_data, the
@@ -238,7 +238,8 @@ def make_lu():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True,
+                    help="the reference checkout (its PGM validation cases are read from it)")
     a = ap.parse_args()
     if not refnet.available():
         raise SystemExit("build the reference oracle first: make -C oracle REF=" + a.ref)
