@@ -3,9 +3,11 @@
 Workload (one "step"): 1024 load scenarios (per-bus lognormal sigma 0.1) of the seeded
 10k-bus transmission-like grid (mean degree 2.8, 10 % tap / phase-shift transformers, 20 % PV,
 2 % shunts), solved together to max |mismatch| < 1e-8 pu: FP32 Jacobian factor and triangular
-solves with one FP64 iterative-refinement step, FP64 mismatch / update / convergence, the
-whole Newton loop on the device (CUDA graph with a device-side while node).  Weak scaling:
-every rank solves its own 1024 scenarios of the same grid.
+solves (two FP64 iterative-refinement steps and factor reuse below 1e-2 pu), FP64 mismatch /
+update / convergence, the whole Newton loop on the device (CUDA graph with a device-side while
+node).  Weak scaling: under torchrun the global batch holds world x 1024 scenarios and each
+rank solves its contiguous shard of 1024 (gap_b200.sharding), with no collective inside the
+Newton loop; statuses are gathered once after the timed region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --workload mixed     # the mixed batch below, one JSON line
@@ -51,8 +53,15 @@ N_SCEN = workloads.N_SCEN
 LARGE_LOAD_SCALE = 0.025
 
 
-def workload(rank: int):
-    return workloads.headline(rank, N_SCEN)
+def workload(rank: int, world: int = 1):
+    """This rank's shard of the global batch: world x N_SCEN scenarios, block b drawn with seed
+    1 + b, split contiguously by sharding.shard (rank r solves block r)."""
+    from gap_b200.sharding import shard
+
+    idx = shard(world * N_SCEN, world, rank)
+    assert idx[0] == rank * N_SCEN and len(idx) == N_SCEN
+    net, s_spec, v0 = workloads.headline(rank, N_SCEN)
+    return net, s_spec, v0, idx
 
 
 def config(extra=None):
@@ -87,7 +96,7 @@ def _cpu_init():
     global _CPU_STATE, _CPU_Y
     from oracle import restate
 
-    _CPU_STATE = workload(0)
+    _CPU_STATE = workload(0)[:3]
     _CPU_Y = restate.ybus_pi(_CPU_STATE[0])
 
 
@@ -248,7 +257,7 @@ def run_ours(args, rank, world, device):
         pool, cores = make_pool()  # spawn context: safe beside the CUDA context
         make_ready(pool, cores)
 
-    net, s_np, v_np = workload(rank)
+    net, s_np, v_np, shard_idx = workload(rank, world)
     zb = float(net.u_rated[0]) ** 2 / BASE
     yp = YbusPlan.from_network(net)
     y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
@@ -283,7 +292,13 @@ def run_ours(args, rank, world, device):
     status = r.status.cpu().numpy()
     iters = r.iterations.cpu().numpy()
     conv = int((status == 0).sum())
-    conv_all = allsum(conv)
+    if dist:
+        from gap_b200.sharding import gather
+
+        full = gather(shard_idx, {"status": status, "iterations": iters}, world * N_SCEN)
+        conv_all = int((full["status"] == 0).sum())
+    else:
+        conv_all = conv
     value = conv_all * args.steps / (ms / 1e3)
 
     # e2e: host (pinned) inputs -> device -> solve -> host results, every step

@@ -20,12 +20,14 @@ POLICY_REFERENCE, POLICY_NEWTON, POLICY_CLAMPED = 0, 1, 2
 JAC_REFERENCE, JAC_EXACT = 0, 1
 ORDER_MINDEG, ORDER_NATURAL = 0, 1
 YBUS_REFERENCE, YBUS_TAPS = 0, 1
+DELTA_REFERENCE, DELTA_FIXED, DELTA_FIXED_TAPS = 0, 1, 2
 SCEN_CONVERGED, SCEN_MAXITER, SCEN_SINGULAR, SCEN_NONFINITE = 0, 1, 2, 3
 
 EXPORTS = [
     "gapk_last_error", "gapk_version", "gapk_device_count",
     "gapk_ybus_create", "gapk_ybus_destroy", "gapk_ybus_nnz", "gapk_ybus_pattern",
-    "gapk_ybus_assemble", "gapk_ybus_apply_changes",
+    "gapk_ybus_assemble", "gapk_ybus_apply_changes", "gapk_ybus_delta_create",
+    "gapk_ybus_delta_destroy", "gapk_ybus_delta_apply",
     "gapk_nr_plan_create", "gapk_nr_plan_destroy", "gapk_nr_plan_get_info",
     "gapk_nr_plan_export",
     "gapk_nr_batch_create", "gapk_nr_batch_destroy", "gapk_nr_batch_device_bytes",
@@ -98,6 +100,10 @@ def lib():
         L.gapk_ybus_assemble.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64,
                                          C.c_void_p, C.c_int64, C.c_int, C.c_double,
                                          C.c_void_p, C.c_int64, C.c_void_p]
+        L.gapk_ybus_delta_apply.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                                            C.c_void_p, C.c_int64, C.c_void_p]
+        L.gapk_ybus_apply_changes.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                              C.c_void_p, C.c_void_p]
         L.gapk_branch_flows.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_int64, C.c_void_p, C.c_double,
                                          C.c_double, C.c_void_p, C.c_void_p, C.c_int,

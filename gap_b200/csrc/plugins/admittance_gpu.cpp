@@ -88,7 +88,10 @@ class B200AdmittanceMatrix final : public gap::admittance::IAdmittanceMatrix {
     // Reference semantics (src/admittance/cpu/cpu_admittance_matrix.cpp:204-301): branch
     // endpoints are taken as matrix indices (shifted down by one when both are positive and
     // one exceeds the matrix size); the first matching CSR entries are updated.  The value
-    // arithmetic runs on the device, in change order.
+    // arithmetic runs on the device, one thread per touched entry, each entry's changes in
+    // change order.  By default the reference's own update, bit for bit (its diagonal delta
+    // carries j b1 + j b1/2, unlike its build); GAP_B200_YBUS_UPDATE=fixed applies the
+    // builder's stamps instead, so that update(build(net)) equals build(changed net).
     std::unique_ptr<gap::SparseMatrix> update_admittance_matrix(
         gap::SparseMatrix const& matrix, std::vector<gap::BranchData> const& changes) override {
         auto Y = std::make_unique<gap::SparseMatrix>(matrix);
@@ -108,15 +111,18 @@ class B200AdmittanceMatrix final : public gap::admittance::IAdmittanceMatrix {
             }
             if (f < 0 || f >= nr || t < 0 || t >= nr) continue;
             pos.insert(pos.end(), {find(f, f), find(t, t), find(f, t), find(t, f)});
-            prm.insert(prm.end(), {ch.r1, ch.x1, ch.g1, ch.b1, ch.status ? 1.0 : 0.0});
+            prm.insert(prm.end(), {ch.r1, ch.x1, ch.g1, ch.b1, 1.0, 0.0, ch.status ? 1.0 : 0.0});
         }
         if (pos.empty() || Y->values.empty()) return Y;
-        int* dpos = d_pos_.upload(pos);
+        const char* env = std::getenv("GAP_B200_YBUS_UPDATE");
+        const int mode = (env && std::string(env) == "fixed") ? GAPK_DELTA_FIXED
+                                                              : GAPK_DELTA_REFERENCE;
         double* dprm = d_branch_.upload(prm);
         double* dv = static_cast<double*>(d_values_.ensure(Y->values.size() * 16));
         check_cuda(cudaMemcpy(dv, Y->values.data(), Y->values.size() * 16, cudaMemcpyHostToDevice),
                    "cudaMemcpy H2D");
-        check(gapk_ybus_apply_changes(static_cast<int>(pos.size() / 4), dpos, dprm, dv, nullptr),
+        check(gapk_ybus_apply_changes(static_cast<int>(pos.size() / 4), pos.data(), dprm, mode, dv,
+                                      nullptr),
               "gapk_ybus_apply_changes");
         check_cuda(cudaMemcpy(Y->values.data(), dv, Y->values.size() * 16, cudaMemcpyDeviceToHost),
                    "cudaMemcpy D2H");
@@ -131,7 +137,7 @@ class B200AdmittanceMatrix final : public gap::admittance::IAdmittanceMatrix {
     gapk_ybus ybus_ = nullptr;
     int n_ = -1;
     std::vector<int> f_, t_, valid_, sb_;
-    DeviceBuffer d_branch_, d_shunt_, d_values_, d_pos_;
+    DeviceBuffer d_branch_, d_shunt_, d_values_;
 };
 
 }  // namespace gapb200

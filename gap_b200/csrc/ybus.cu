@@ -11,8 +11,10 @@
 // r*r + x*x with two roundings.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/gapk.h"
@@ -100,15 +102,22 @@ __global__ void k_ybus(int nnz, int n_scen, const int* __restrict__ slot_src,
     out[(size_t)s * out_stride + p] = make_double2(vr, vi);
 }
 
-// Branch status changes applied to existing values, in change order (one thread: the deltas
-// of different changes may hit the same entry, and the reference applies them sequentially,
-// src/admittance/cpu/cpu_admittance_matrix.cpp:214-297).  pos = (diag f, diag t, (f,t), (t,f))
-// CSR indices or -1; prm = (r1, x1, g1, b1, status).
-__global__ void k_ybus_changes(int n, const int* __restrict__ pos, const double* __restrict__ prm,
-                               double2* values) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    for (int i = 0; i < n; ++i) {
-        const double* q = prm + (size_t)i * 5;
+// Branch status changes on existing values, one thread per (scenario, touched CSR slot).
+// Each thread applies the deltas of its slot in change order, so the result of every slot is
+// the one the reference's sequential loop gives (src/admittance/cpu/cpu_admittance_matrix.cpp:
+// 214-297: different slots never interact), whatever the number of threads.
+//   item  = (scenario, slot, first, last) into seg; seg[e] = change index << 2 | role, role
+//           0 / 1 the from / to diagonal, 2 the (from, to) entry, 3 the (to, from) entry
+//   prm   = (r1, x1, g1, b1, k, theta, status) per change, Ohm / S
+// Delta of one change (sign + when the branch comes into service, - when it leaves):
+//   GAPK_DELTA_REFERENCE   the reference's update: diagonals y + g1 + j b1 + j b1/2 (unlike its
+//                          build, which stamps y + g1 + j b1/2), off-diagonals -y; taps ignored
+//   GAPK_DELTA_FIXED       the builder's own stamps, taps ignored (GAPK_YBUS_REFERENCE)
+//   GAPK_DELTA_FIXED_TAPS  the builder's pi-model stamps with the tap (GAPK_YBUS_TAPS)
+// scale multiplies every delta (1 = Siemens, Z_base = per unit).
+__device__ __forceinline__ double2 change_delta(const double* __restrict__ q, int role, int mode) {
+    double2 d;
+    if (mode == GAPK_DELTA_REFERENCE) {
         const double r = q[0], x = q[1], g = q[2], b = q[3];
         const double z2 = __dadd_rn(__dmul_rn(r, r), __dmul_rn(x, x));
         double yr = 0.0, yi = 0.0;
@@ -116,32 +125,45 @@ __global__ void k_ybus_changes(int n, const int* __restrict__ pos, const double*
             yr = __ddiv_rn(r, z2);
             yi = __ddiv_rn(-x, z2);
         }
-        // total = series + (g1 + j b1); the diagonals also get j b1/2 (the reference's
-        // update adds both, unlike its build)
-        double tr = __dadd_rn(yr, g), ti = __dadd_rn(yi, b);
-        double sr = 0.0, si = __ddiv_rn(b, 2.0);
-        double orr = yr, oi = yi;
-        if (q[4] == 0.0) {
-            tr = -tr;
-            ti = -ti;
-            si = -si;
-            orr = -orr;
-            oi = -oi;
-            sr = -sr;
+        if (role < 2) {
+            // (y + (g1 + j b1)) + j b1/2, each sum rounded as the reference's complex adds
+            d = make_double2(__dadd_rn(__dadd_rn(yr, g), 0.0),
+                             __dadd_rn(__dadd_rn(yi, b), __ddiv_rn(b, 2.0)));
+        } else {
+            d = make_double2(-yr, -yi);
         }
-        const double dr = __dadd_rn(tr, sr), di = __dadd_rn(ti, si);
-        const int* p = pos + (size_t)i * 4;
-        for (int k = 0; k < 2; ++k)
-            if (p[k] >= 0) {
-                double2 v = values[p[k]];
-                values[p[k]] = make_double2(__dadd_rn(v.x, dr), __dadd_rn(v.y, di));
-            }
-        for (int k = 2; k < 4; ++k)
-            if (p[k] >= 0) {
-                double2 v = values[p[k]];
-                values[p[k]] = make_double2(__dsub_rn(v.x, orr), __dsub_rn(v.y, oi));
-            }
+    } else {
+        const Stamps st = branch_stamps(q, mode == GAPK_DELTA_FIXED ? GAPK_YBUS_REFERENCE
+                                                                    : GAPK_YBUS_TAPS);
+        d = role == 0 ? st.ff : role == 1 ? st.tt : role == 2 ? st.ft : st.tf;
     }
+    if (q[6] == 0.0) d = make_double2(-d.x, -d.y);
+    return d;
+}
+
+__global__ void k_ybus_delta(int n_items, const int4* __restrict__ items,
+                             const int* __restrict__ seg, const double* __restrict__ prm,
+                             int mode, double scale, double2* __restrict__ values,
+                             long long stride) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_items) return;
+    const int4 it = items[t];
+    double2* v = values + (size_t)it.x * stride + it.y;
+    double vr = v->x, vi = v->y;
+    for (int e = it.z; e < it.w; ++e) {
+        const int c = seg[e] >> 2, role = seg[e] & 3;
+        double2 d = change_delta(prm + (size_t)c * 7, role, mode);
+        if (scale != 1.0) d = make_double2(__dmul_rn(d.x, scale), __dmul_rn(d.y, scale));
+        if (mode == GAPK_DELTA_REFERENCE && role >= 2) {
+            // values[idx] -= series change: -(+-y)
+            vr = __dsub_rn(vr, -d.x);
+            vi = __dsub_rn(vi, -d.y);
+        } else {
+            vr = __dadd_rn(vr, d.x);
+            vi = __dadd_rn(vi, d.y);
+        }
+    }
+    *v = make_double2(vr, vi);
 }
 
 }  // namespace
@@ -294,21 +316,131 @@ int gapk_ybus_assemble(gapk_ybus y, int n_scen, const double* d_branch, int64_t 
     return GAPK_OK;
 }
 
-int gapk_ybus_apply_changes(int n_changes, const int* d_pos, const double* d_params,
+}  // extern "C"
+
+// Segmented plan of branch changes: for every scenario, the CSR slots its changes touch, each
+// with its (change, role) list in change order.
+struct gapk_ybus_delta_s {
+    int n_scen = 0, n_changes = 0;
+    std::vector<int> items;  // int4 per (scenario, slot): scenario, slot, seg begin, seg end
+    std::vector<int> seg;
+    int device = -1;
+    void* d_items = nullptr;
+    void* d_seg = nullptr;
+    ~gapk_ybus_delta_s() {
+        if (d_items) cudaFree(d_items);
+        if (d_seg) cudaFree(d_seg);
+    }
+    int upload() {
+        if (d_items || items.empty()) return GAPK_OK;
+        cudaError_t e = cudaMalloc(&d_items, items.size() * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&d_seg, std::max<size_t>(seg.size(), 1) * sizeof(int));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(d_items, items.data(), items.size() * sizeof(int), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !seg.empty())
+            e = cudaMemcpy(d_seg, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            set_error(std::string("ybus delta upload: ") + cudaGetErrorString(e));
+            return e == cudaErrorMemoryAllocation ? GAPK_ENOMEM : GAPK_ECUDA;
+        }
+        cudaGetDevice(&device);
+        return GAPK_OK;
+    }
+};
+
+namespace {
+
+int delta_build(int n_scen, const int* change_ptr, const int* pos, gapk_ybus_delta_s& d) {
+    d.n_scen = n_scen;
+    d.n_changes = change_ptr[n_scen];
+    std::vector<std::pair<int, int>> touch;  // (slot, change << 2 | role), per scenario
+    for (int s = 0; s < n_scen; ++s) {
+        if (change_ptr[s + 1] < change_ptr[s]) return GAPK_EINVAL;
+        touch.clear();
+        for (int c = change_ptr[s]; c < change_ptr[s + 1]; ++c)
+            for (int r = 0; r < 4; ++r)
+                if (pos[4 * c + r] >= 0) touch.emplace_back(pos[4 * c + r], c << 2 | r);
+        // by slot; within a slot in change order (stable: the list is built in change order)
+        std::stable_sort(touch.begin(), touch.end(),
+                         [](auto const& a, auto const& b) { return a.first < b.first; });
+        for (size_t i = 0; i < touch.size();) {
+            size_t j = i;
+            while (j < touch.size() && touch[j].first == touch[i].first) ++j;
+            d.items.insert(d.items.end(), {s, touch[i].first, static_cast<int>(d.seg.size()),
+                                           static_cast<int>(d.seg.size() + (j - i))});
+            for (size_t k = i; k < j; ++k) d.seg.push_back(touch[k].second);
+            i = j;
+        }
+    }
+    return GAPK_OK;
+}
+
+int delta_launch(gapk_ybus_delta_s& d, const double* d_params, int mode, double scale,
+                 double* d_values, int64_t stride, cudaStream_t st) {
+    int rc = d.upload();
+    if (rc) return rc;
+    const int n_items = static_cast<int>(d.items.size() / 4);
+    if (n_items == 0) return GAPK_OK;
+    k_ybus_delta<<<(n_items + 255) / 256, 256, 0, st>>>(
+        n_items, static_cast<const int4*>(d.d_items), static_cast<const int*>(d.d_seg), d_params,
+        mode, scale, reinterpret_cast<double2*>(d_values), stride);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("k_ybus_delta launch: ") + cudaGetErrorString(e));
+        return GAPK_ECUDA;
+    }
+    return GAPK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gapk_ybus_delta_create(int n_scen, const int* h_change_ptr, const int* h_pos,
+                           gapk_ybus_delta* out) {
+    if (!out || n_scen <= 0 || !h_change_ptr || h_change_ptr[0] != 0 ||
+        (h_change_ptr[n_scen] > 0 && !h_pos)) {
+        set_error("gapk_ybus_delta_create: bad arguments");
+        return GAPK_EINVAL;
+    }
+    auto d = std::make_unique<gapk_ybus_delta_s>();
+    if (delta_build(n_scen, h_change_ptr, h_pos, *d)) {
+        set_error("gapk_ybus_delta_create: change_ptr must be non-decreasing");
+        return GAPK_EINVAL;
+    }
+    *out = d.release();
+    return GAPK_OK;
+}
+
+int gapk_ybus_delta_destroy(gapk_ybus_delta d) {
+    delete d;
+    return GAPK_OK;
+}
+
+int gapk_ybus_delta_apply(gapk_ybus_delta d, const double* d_params, int mode, double scale,
+                          double* d_values, int64_t values_stride, void* stream) {
+    if (!d || !d_values ||
+        (mode != GAPK_DELTA_REFERENCE && mode != GAPK_DELTA_FIXED &&
+         mode != GAPK_DELTA_FIXED_TAPS) ||
+        (d->n_changes > 0 && !d_params) || (d->n_scen > 1 && values_stride <= 0)) {
+        set_error("gapk_ybus_delta_apply: bad arguments");
+        return GAPK_EINVAL;
+    }
+    return delta_launch(*d, d_params, mode, scale, d_values, values_stride,
+                        static_cast<cudaStream_t>(stream));
+}
+
+int gapk_ybus_apply_changes(int n_changes, const int* h_pos, const double* d_params, int mode,
                             double* d_values, void* stream) {
-    if (n_changes < 0 || (n_changes > 0 && (!d_pos || !d_params || !d_values))) {
+    if (n_changes < 0 || (n_changes > 0 && (!h_pos || !d_params || !d_values))) {
         set_error("gapk_ybus_apply_changes: bad arguments");
         return GAPK_EINVAL;
     }
     if (n_changes == 0) return GAPK_OK;
-    k_ybus_changes<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(
-        n_changes, d_pos, d_params, reinterpret_cast<double2*>(d_values));
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        set_error(std::string("k_ybus_changes launch: ") + cudaGetErrorString(e));
-        return GAPK_ECUDA;
-    }
-    return GAPK_OK;
+    const int ptr[2] = {0, n_changes};
+    gapk_ybus_delta_s d;
+    if (delta_build(1, ptr, h_pos, d)) return GAPK_EINVAL;
+    return gapk_ybus_delta_apply(&d, d_params, mode, 1.0, d_values, 0, stream);
 }
 
 int gapk_branch_flows(int n_scen, int n_bus, int n_branch, const int* d_from, const int* d_to,

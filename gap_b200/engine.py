@@ -60,6 +60,7 @@ class YbusPlan:
         sb = N.i32(shunt_bus)
         self.n_branch = int(f.size)
         self.n_shunt = int(sb.size)
+        self.from_idx, self.to_idx, self.in_service = f, t, s
         h = C.c_void_p()
         N.check(L.gapk_ybus_create(C.c_int(self.n_bus), C.c_int(self.n_branch), N.iptr(f),
                                    N.iptr(t), N.iptr(s), C.c_int(self.n_shunt), N.iptr(sb),
@@ -95,10 +96,92 @@ class YbusPlan:
                                            _stream_ptr(stream)))
         return out
 
+    def branch_positions(self) -> np.ndarray:
+        """[n_branch, 4] int32: the CSR indices of each in-service branch's own stamps
+        (diagonal from, diagonal to, (from, to), (to, from)); -1 rows for out-of-service
+        branches.  The pattern keeps the duplicates of parallel branches, in branch order
+        (src/admittance/cpu/cpu_admittance_matrix.cpp:151-186), so the k-th branch joining
+        two buses owns the k-th duplicate of their off-diagonal entries."""
+        rp, ci = self.row_ptr, self.col_idx
+        out = np.full((self.n_branch, 4), -1, np.int32)
+        diag = np.full(self.n_bus, -1, np.int64)
+        rows = np.repeat(np.arange(self.n_bus), np.diff(rp))
+        d = np.nonzero(ci == rows)[0]
+        diag[rows[d][::-1]] = d[::-1]  # first diagonal entry of each row
+        seen = {}
+        for b in range(self.n_branch):
+            if not self.in_service[b]:
+                continue
+            f, t = int(self.from_idx[b]), int(self.to_idx[b])
+            if f == t:
+                raise ValueError(f"branch {b} connects bus {f} to itself")
+            out[b, 0], out[b, 1] = diag[f], diag[t]
+            for role, (r, c) in ((2, (f, t)), (3, (t, f))):
+                k = seen.get((r, c), 0)
+                seen[(r, c)] = k + 1
+                hits = rp[r] + np.nonzero(ci[rp[r]:rp[r + 1]] == c)[0]
+                out[b, role] = hits[k]
+        return out
+
     def __del__(self):
         try:
             if self._h:
                 N.lib().gapk_ybus_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class YbusDelta:
+    """Branch status changes for a batch of scenarios on one Y pattern, applied on the device
+    one thread per touched entry (gapk_ybus_delta_*; the reference applies one change list
+    sequentially, src/admittance/cpu/cpu_admittance_matrix.cpp:204-301).
+
+    changes: one list of branch indices per scenario.  positions: [n_branch, 4] CSR indices
+    per branch (default: each branch's own entries, YbusPlan.branch_positions)."""
+
+    MODES = {"reference": N.DELTA_REFERENCE, "fixed": N.DELTA_FIXED,
+             "fixed_taps": N.DELTA_FIXED_TAPS}
+
+    def __init__(self, yplan: YbusPlan, changes, positions=None):
+        pos = yplan.branch_positions() if positions is None else np.asarray(positions, np.int32)
+        self.branches = [np.asarray(c, np.int64).reshape(-1) for c in changes]
+        self.n_scen = len(self.branches)
+        ptr = np.zeros(self.n_scen + 1, np.int32)
+        ptr[1:] = np.cumsum([len(c) for c in self.branches])
+        flat = np.concatenate(self.branches) if ptr[-1] else np.zeros(0, np.int64)
+        self.change_branch = flat
+        hp = N.i32(pos[flat].reshape(-1)) if len(flat) else np.zeros(4, np.int32)
+        h = C.c_void_p()
+        N.check(N.lib().gapk_ybus_delta_create(C.c_int(self.n_scen), N.iptr(ptr), N.iptr(hp),
+                                               C.byref(h)))
+        self._h = h
+        self.nnz = yplan.nnz
+
+    def params(self, branch: np.ndarray, status) -> np.ndarray:
+        """[n_changes, 7] (r1, x1, g1, b1, k, theta, status) from branch_params rows and the
+        new status per change (scalar or [n_changes])."""
+        prm = np.zeros((len(self.change_branch), 7))
+        prm[:, :6] = np.asarray(branch)[self.change_branch]
+        prm[:, 6] = status
+        return prm
+
+    def apply(self, values, params, mode="fixed_taps", scale=1.0, stream=None):
+        """values: complex128 [n_scen, nnz] on the device, changed in place; params: float64
+        [n_changes, 7] (device tensor or host array)."""
+        torch = _torch()
+        prm = torch.as_tensor(np.asarray(params, np.float64) if not torch.is_tensor(params)
+                              else params, device=values.device).contiguous()
+        N.check(N.lib().gapk_ybus_delta_apply(self._h, _dptr(prm), self.MODES[mode],
+                                              float(scale), _dptr(values),
+                                              values.stride(0) if values.dim() == 2 else 0,
+                                              _stream_ptr(stream)))
+        return values
+
+    def __del__(self):
+        try:
+            if self._h:
+                N.lib().gapk_ybus_delta_destroy(self._h)
                 self._h = None
         except Exception:
             pass

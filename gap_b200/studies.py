@@ -6,10 +6,11 @@ CUDA stream, with the Newton loop of every study captured once as a CUDA graph:
 
 * load scenarios of one grid: one Y shared by every scenario, per-scenario S_spec;
 * N-1 branch contingencies of one grid: the grid's own Y pattern, one Y value set per
-  scenario in which the outaged branch has r1 = x1 = g1 = b1 = 0.  The Y-bus builder stamps
-  a branch with |z|^2 <= 1e-12 as zero admittance (src/admittance/cpu/
-  cpu_admittance_matrix.cpp:120-128), so the outage leaves explicit zeros in place of the
-  branch's entries and every contingency shares the base grid's symbolic analysis;
+  scenario: the base values with the outaged branch's stamps removed on the device (a
+  batched, fixed version of the reference's update_admittance_matrix,
+  src/admittance/cpu/cpu_admittance_matrix.cpp:204-301), so the outage leaves (near-)zeros in
+  place of the branch's entries and every contingency shares the base grid's symbolic
+  analysis;
 * independent grids: one study per grid.
 
 `autotune` picks the scenario-lane count and the thread count of the level-scheduled kernels
@@ -25,7 +26,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
-from .engine import NRBatch, NRPlan, NRResult, YbusPlan, branch_params, shunt_params
+from .engine import (NRBatch, NRPlan, NRResult, YbusDelta, YbusPlan, branch_params,
+                     shunt_params)
 from .network import Network
 
 
@@ -121,12 +123,19 @@ def load_study(name, net: Network, s_spec, v0, base_power=1e8, precision="fp32",
 
 def contingency_study(name, net: Network, outages, s_spec, v0, base_power=1e8,
                       precision="fp32", plan: NRPlan | None = None) -> Study:
-    """N-1 branch outages of one grid, one scenario per outage, sharing the grid's plan."""
+    """N-1 branch outages of one grid, one scenario per outage, sharing the grid's plan.  The
+    scenarios' Y values are the base grid's with the outaged branch's stamps removed on the
+    device (YbusDelta, builder's pi-model stamps): its entries stay in the pattern as
+    (near-)zeros, so every scenario keeps the base symbolic analysis."""
     torch = _torch()
-    yp, y = _ybus(net, base_power, branch=contingency_branch_params(net, outages))
+    yp, y0 = _ybus(net, base_power)
     if plan is None:
         plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
     S = len(outages)
+    y = y0.repeat(S, 1).contiguous()
+    delta = YbusDelta(yp, [[int(b)] for b in outages])
+    zb = float(net.u_rated[0]) ** 2 / base_power
+    delta.apply(y, delta.params(branch_params(net), 0.0), mode="fixed_taps", scale=zb)
     s = np.asarray(s_spec, np.complex128)
     if s.ndim == 1:
         s = np.repeat(s[None], S, axis=0)

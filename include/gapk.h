@@ -95,11 +95,40 @@ int gapk_ybus_assemble(gapk_ybus y, int n_scen, const double* d_branch, int64_t 
                        double* d_values, int64_t values_stride, void* stream);
 
 /* Branch status changes on existing Y values (IAdmittanceMatrix::update_admittance_matrix,
- * src/admittance/cpu/cpu_admittance_matrix.cpp:204-301), applied on the device in change
- * order.  d_pos[i*4..] = CSR indices of (diag from, diag to, (from,to), (to,from)) or -1, as
- * the caller located them in the pattern; d_params[i*5..] = (r1, x1, g1, b1, status). */
-int gapk_ybus_apply_changes(int n_changes, const int* d_pos, const double* d_params,
+ * include/gap/admittance/admittance_interface.h:24-31; reference semantics
+ * src/admittance/cpu/cpu_admittance_matrix.cpp:204-301).  A change sets one branch's status:
+ * its stamps are added (status 1) or removed (status 0).  Changes are applied per CSR slot in
+ * change order, one device thread per touched slot, so the result equals the sequential
+ * application's.
+ *   h_pos[i*4..]    : CSR indices of (diag from, diag to, (from,to), (to,from)) or -1, as
+ *                     located in the pattern by the caller (host memory)
+ *   d_params[i*7..] : (r1, x1, g1, b1, k, theta, status) in Ohm / S (device)
+ *   mode            : GAPK_DELTA_REFERENCE  the reference's update, bit for bit: diagonals
+ *                                           change by y + g1 + j b1 + j b1/2 (its build stamps
+ *                                           y + g1 + j b1/2), taps ignored
+ *                     GAPK_DELTA_FIXED      the builder's own stamps (y + g1 + j b1/2), taps
+ *                                           ignored: update(build(net)) = build(changed net)
+ *                     GAPK_DELTA_FIXED_TAPS the builder's pi-model stamps with the tap
+ *                                           (GAPK_YBUS_TAPS)
+ * gapk_ybus_apply_changes applies one change list to one value vector; the delta plan below
+ * applies per-scenario change lists to a batch. */
+#define GAPK_DELTA_REFERENCE 0
+#define GAPK_DELTA_FIXED 1
+#define GAPK_DELTA_FIXED_TAPS 2
+int gapk_ybus_apply_changes(int n_changes, const int* h_pos, const double* d_params, int mode,
                             double* d_values, void* stream);
+
+/* Batched branch changes (no reference counterpart; contingency screening): scenario s applies
+ * changes h_change_ptr[s] .. h_change_ptr[s+1]-1 (positions h_pos as above) to its own value
+ * vector d_values + s * values_stride (complex entries), every delta multiplied by scale
+ * (1 = Siemens, Z_base = per unit).  The plan (the touched slots of every scenario, each with
+ * its changes in order) is built once on the host and reused for any parameters. */
+typedef struct gapk_ybus_delta_s* gapk_ybus_delta;
+int gapk_ybus_delta_create(int n_scen, const int* h_change_ptr, const int* h_pos,
+                           gapk_ybus_delta* out);
+int gapk_ybus_delta_destroy(gapk_ybus_delta d);
+int gapk_ybus_delta_apply(gapk_ybus_delta d, const double* d_params, int mode, double scale,
+                          double* d_values, int64_t values_stride, void* stream);
 
 /* Branch results of solved scenarios: fills, per scenario and branch, the BranchData result
  * fields p_from, q_from, i_from, s_from, p_to, q_to, i_to, s_to, loading

@@ -545,6 +545,47 @@ def ybus_update_reference(Y, changes: Network):
     return row_ptr, col_idx, out
 
 
+def change_stamps(prm, taps):
+    """The Y-bus builder's four stamps (ff, tt, ft, tf) of one branch, prm = (r1, x1, g1, b1,
+    k, theta, ...): y = 1/(r + jx) (0 when |z|^2 <= 1e-12), end stamp y + g1 + j b1/2
+    (cpu_admittance_matrix.cpp:120-139), and with taps the pi model of ybus_pi."""
+    r, x, g, b, kk, th = (float(v) for v in prm[:6])
+    z2 = r * r + x * x
+    yr, yi = (r / z2, -x / z2) if z2 > 1e-12 else (0.0, 0.0)
+    end = complex((yr + g) + 0.0, (yi + 0.0) + b / 2.0)
+    y = complex(yr, yi)
+    if not taps or (kk == 1.0 and th == 0.0):
+        return end, end, -y, -y
+    tap = kk * complex(math.cos(th), math.sin(th))
+    return end / (kk * kk), end, -y / tap.conjugate(), -y / tap
+
+
+def ybus_delta(values, positions, params, mode, scale=1.0):
+    """Branch status changes applied to Y values in change order (the batched device update's
+    restatement).  positions [c, 4] = CSR indices (diag from, diag to, (from,to), (to,from)) or
+    -1; params [c, 7] = (r1, x1, g1, b1, k, theta, status).  mode 'reference': the reference's
+    update (cpu_admittance_matrix.cpp:238-297: diagonals y + g1 + j b1 + j b1/2, off-diagonals
+    -y, taps ignored); 'fixed': the builder's stamps without taps; 'fixed_taps': with taps.
+    Deltas are added for status 1 and subtracted for status 0, multiplied by scale."""
+    out = np.array(values, np.complex128).copy()
+    for c in range(len(params)):
+        q = params[c]
+        if mode == "reference":
+            r, x, g, b = (float(v) for v in q[:4])
+            z2 = r * r + x * x
+            ys = complex(r / z2, -x / z2) if z2 > 1e-12 else 0j
+            diag = (ys + complex(g, b)) + complex(0.0, b / 2.0)
+            d = (diag, diag, -ys, -ys)
+        else:
+            d = change_stamps(q, taps=(mode == "fixed_taps"))
+        sign = 1.0 if q[6] != 0.0 else -1.0
+        for role in range(4):
+            p = int(positions[c][role])
+            if p >= 0:
+                out[p] += sign * d[role] * scale
+    return out
+
+
 def branch_flows(net: Network, v, base_power, i_n=None, sn=None, taps=True):
     """Branch results of a solved network, in the units of the reference's BranchData result
     fields (include/gap/core/types.h:233-243: p/q in W/var, s in VA, i in A, loading), which

@@ -132,3 +132,33 @@ def random_network(seed, n_max=40):
                          from_id=ids[frm], to_id=ids[to], r1=r, x1=x, b1=b, k=k, theta=th,
                          status=status, app_node=app_node, app_type=app_type, app_g1=app_g1,
                          app_b1=app_b1)
+
+
+def with_parallel_branches(net, branches, reverse=()):
+    """Copy of `net` with a duplicate of each listed branch appended (new ids; the copies of
+    the branches in `reverse` run to -> from), so that the Y pattern holds duplicate entries."""
+    import dataclasses
+
+    branches = list(branches)
+    rev = np.isin(branches, list(reverse))
+    kw = {}
+    for name in ("r1", "x1", "g1", "b1", "k", "theta", "status"):
+        a = getattr(net, name)
+        kw[name] = np.concatenate([a, a[branches]])
+    f = net.from_id[branches]
+    t = net.to_id[branches]
+    kw["from_id"] = np.concatenate([net.from_id, np.where(rev, t, f)]).astype(net.from_id.dtype)
+    kw["to_id"] = np.concatenate([net.to_id, np.where(rev, f, t)]).astype(net.to_id.dtype)
+    start = int(max(np.max(net.br_id), np.max(net.bus_id), np.max(net.app_id, initial=0))) + 1
+    kw["br_id"] = np.concatenate([net.br_id, np.arange(start, start + len(branches))]).astype(
+        net.br_id.dtype)
+    return dataclasses.replace(net, **kw)
+
+
+def dense_of(Y):
+    """CSR (row_ptr, col_idx, values) with duplicates summed, as a dense complex matrix."""
+    import scipy.sparse as sp
+
+    rp, ci, va = Y
+    n = len(rp) - 1
+    return sp.csr_matrix((np.array(va), np.array(ci), np.array(rp)), shape=(n, n)).toarray()

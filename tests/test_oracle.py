@@ -266,3 +266,55 @@ def test_pgm_writer_components_and_balances():
     gb = out["generic_branch"][0]
     assert gb["loading"] == pytest.approx(max(gb["i_from"], gb["i_to"]) / extra["i_n"][2],
                                           rel=1e-12)
+
+
+def test_ybus_delta_fixed_restatement_equals_fresh_build():
+    """The fixed update (the builder's own stamps) takes build(net) to build(changed net):
+    branch outages, a parallel pair (one reversed) and a re-closure in one change list, with
+    and without taps, within 1e-14 of the largest entry."""
+    import dataclasses
+
+    from gap_b200 import synth
+    from gap_b200.engine import YbusPlan, branch_params
+    from helpers import dense_of, with_parallel_branches
+
+    net = with_parallel_branches(synth.transmission_grid(2, n=300), [0, 5, 9], reverse=[5])
+    m0 = net.n_branch - 3
+    yp = YbusPlan.from_network(net)
+    pos = yp.branch_positions()
+    changes = [3, 5, m0 + 1, 9, 3]  # out, out, out (parallel to 5), out, back in
+    status = [0, 0, 0, 0, 1]
+    prm = np.zeros((len(changes), 7))
+    prm[:, :6] = branch_params(net)[changes]
+    prm[:, 6] = status
+    st = net.status.copy()
+    for b, s in zip(changes, status):
+        st[b] = s
+    changed = dataclasses.replace(net, status=st)
+    for mode, build in (("fixed_taps", restate.ybus_pi), ("fixed", restate.ybus_reference)):
+        base = build(net)
+        rp, ci, va = base
+        assert np.array_equal(rp, yp.row_ptr) and np.array_equal(ci, yp.col_idx)
+        upd = restate.ybus_delta(va, pos[changes], prm, mode)
+        a, b = dense_of((rp, ci, upd)), dense_of(build(changed))
+        assert np.max(np.abs(a - b)) <= 1e-14 * np.max(np.abs(b)), mode
+
+
+def test_ybus_delta_reference_restatement_matches_reference_update():
+    """The batched update's reference mode, restated, against the reference's own update."""
+    d = load("kat_update")
+    net = net_from(d)
+    ch = net_from(d, "ch_")
+    Y = restate.ybus_reference(net)
+    rp, ci, va = Y
+    pos, prm = [], []
+    for b in range(ch.n_branch):
+        f, t = int(ch.from_id[b]), int(ch.to_id[b])
+
+        def find(r, c):
+            hit = np.nonzero(ci[rp[r]:rp[r + 1]] == c)[0]
+            return int(rp[r] + hit[0]) if len(hit) else -1
+        pos.append([find(f, f), find(t, t), find(f, t), find(t, f)])
+        prm.append([ch.r1[b], ch.x1[b], ch.g1[b], ch.b1[b], 1.0, 0.0, float(ch.status[b])])
+    out = restate.ybus_delta(va, np.array(pos), np.array(prm), "reference")
+    np.testing.assert_allclose(out, d["y_values"], rtol=1e-14, atol=1e-14)
