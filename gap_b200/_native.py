@@ -31,7 +31,8 @@ EXPORTS = [
     "gapk_nr_plan_create", "gapk_nr_plan_destroy", "gapk_nr_plan_get_info",
     "gapk_nr_plan_export",
     "gapk_nr_batch_create", "gapk_nr_batch_destroy", "gapk_nr_batch_device_bytes",
-    "gapk_nr_solve", "gapk_nr_last_loop_count",
+    "gapk_nr_solve", "gapk_nr_last_loop_count", "gapk_nr_mix_create", "gapk_nr_mix_destroy",
+    "gapk_nr_mix_solve",
     "gapk_nr_stage_load", "gapk_nr_stage_mismatch", "gapk_nr_stage_jacobian",
     "gapk_nr_stage_factor", "gapk_nr_stage_solve", "gapk_nr_stage_get_correction",
     "gapk_nr_stage_get_mismatch", "gapk_nr_stage_kernel", "gapk_nr_solve_noalloc",
@@ -104,6 +105,7 @@ def lib():
                                             C.c_void_p, C.c_int64, C.c_void_p]
         L.gapk_ybus_apply_changes.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                               C.c_void_p, C.c_void_p]
+        L.gapk_nr_mix_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         L.gapk_branch_flows.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_int64, C.c_void_p, C.c_double,
                                          C.c_double, C.c_void_p, C.c_void_p, C.c_int,

@@ -75,6 +75,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             print(" ".join(cmd))
         _run(cmd)
     build_plugins(so, verbose=verbose, force=force)
+    build_io_and_cli(verbose=verbose, force=force)
     return so
 
 
@@ -99,6 +100,32 @@ def build_plugins(core_so, verbose=False, force=False):
             if verbose:
                 print(" ".join(cmd))
             _run(cmd)
+
+
+def build_io_and_cli(verbose=False, force=False):
+    """libgap_io_pgm.so (the PGM reader behind the reference's IIOModule; host code only) and
+    gap_b200_main (the reference's command-line flow over the B200 libraries, which it loads
+    with dlopen through an $ORIGIN rpath)."""
+    pdir = os.path.join(HERE, "plugins")
+    iface = os.path.join(INCLUDE, "gap_b200", "gap_interfaces.hpp")
+    # nvcc's host compiler, as for the plugin libraries (one C++ runtime for every library)
+    cxx = [_nvcc(), "-x", "c++", "-cudart", "none"]
+    io_src = os.path.join(pdir, "pgm_io.cpp")
+    io_so = os.path.join(LIB, "libgap_io_pgm.so")
+    if force or _stale(io_so, [io_src, iface, os.path.join(pdir, "json_min.hpp")]):
+        cmd = cxx + ["-std=c++20", "-O2", "-Xcompiler", "-fPIC", "-shared", "-I" + INCLUDE, "-o",
+                     io_so, io_src]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    cli_src = os.path.join(pdir, "gap_b200_main.cpp")
+    cli = os.path.join(LIB, "gap_b200_main")
+    if force or _stale(cli, [cli_src, iface]):
+        cmd = cxx + ["-std=c++20", "-O2", "-I" + INCLUDE, "-o", cli, cli_src, "-ldl",
+                     "-Xlinker", "-rpath=$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
 
 
 if __name__ == "__main__":

@@ -183,7 +183,7 @@ void launch_solve(gapk_nr_batch b, cudaStream_t st, const double2* rhs, double2*
     BatchDev const& B = b->dev;
     k_solve_fwd<T, SW><<<b->G, b->threads, 0, st>>>(P, B, rhs, acc);
     if (P.n_tail > 0)
-        k_dense_solve<T, SW><<<b->G * SW, 256, 2 * P.n_tail * sizeof(T), st>>>(P, B, out, acc);
+        k_dense_solve<T, SW><<<b->G * SW, 256, dense_solve_smem(P.n_tail, sizeof(T)), st>>>(P, B, out, acc);
     k_solve_bwd<T, SW><<<b->G, b->threads, 0, st>>>(P, B, out, acc);
 }
 
@@ -207,8 +207,7 @@ void launch_body(gapk_nr_batch b, cudaStream_t st, int use_cond, cudaGraphCondit
     PlanDev const& P = b->plan->dev;
     BatchDev const& B = b->dev;
     const int G = b->G;
-    dim3 gm(blocks_for((long)P.n_bus * SW, 256), G);
-    k_mismatch<SW><<<gm, 256, 0, st>>>(P, B);
+    k_mismatch<SW><<<mismatch_grid<SW>(P, G), 256, 0, st>>>(P, B);
     k_check<SW><<<1, 1024, 0, st>>>(B, use_cond, h);
     dim3 gj(blocks_for((long)P.n_a * SW, 256), G);
     k_jfill<T, SW><<<gj, 256, 0, st>>>(P, B);
@@ -290,11 +289,9 @@ struct StageOp {
         BatchDev const& B = b->dev;
         const int G = b->G;
         switch (which) {
-            case 0: {
-                dim3 gm(blocks_for((long)P.n_bus * SW, 256), G);
-                k_mismatch<SW><<<gm, 256, 0, st>>>(P, B);
+            case 0:
+                k_mismatch<SW><<<mismatch_grid<SW>(P, G), 256, 0, st>>>(P, B);
                 break;
-            }
             case 1: {
                 dim3 gj(blocks_for((long)P.n_a * SW, 256), G);
                 k_jfill<T, SW><<<gj, 256, 0, st>>>(P, B);
@@ -326,7 +323,7 @@ struct KernelOp {
         BatchDev const& B = b->dev;
         const int G = b->G;
         switch (which) {
-            case 0: k_mismatch<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B); break;
+            case 0: k_mismatch<SW><<<mismatch_grid<SW>(P, G), 256, 0, st>>>(P, B); break;
             case 1: k_jfill<T, SW><<<dim3(blocks_for((long)P.n_a * SW, 256), G), 256, 0, st>>>(P, B); break;
             case 2: k_factor<T, SW><<<G, b->threads, 0, st>>>(P, B); break;
             case 3:
@@ -343,7 +340,7 @@ struct KernelOp {
             case 5: k_solve_fwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs, 0); break;
             case 6:
                 if (P.n_tail > 0)
-                    k_dense_solve<T, SW><<<G * SW, 256, 2 * P.n_tail * sizeof(T), st>>>(P, B, B.dx, 0);
+                    k_dense_solve<T, SW><<<G * SW, 256, dense_solve_smem(P.n_tail, sizeof(T)), st>>>(P, B, B.dx, 0);
                 break;
             case 7: k_solve_bwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.dx, 0); break;
             case 8: k_update<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B); break;
@@ -368,7 +365,7 @@ struct AdjointOp {
         BatchDev const& B = b->dev;
         const int G = b->G;
         k_adj_prep<SW><<<blocks_for((long)G * SW, 256), 256, 0, st>>>(B);
-        k_mismatch<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B);
+        k_mismatch<SW><<<mismatch_grid<SW>(P, G), 256, 0, st>>>(P, B);
         k_jfill<T, SW><<<dim3(blocks_for((long)P.n_a * SW, 256), G), 256, 0, st>>>(P, B);
         launch_factor<T, SW>(b, st);
         k_adj_rhs<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B, dvm, dva);
@@ -461,6 +458,31 @@ int build_graph(gapk_nr_batch b, cudaStream_t st) {
     GAPK_CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
     b->graph_refine = b->cur_refine;
     (void)st;
+    return GAPK_OK;
+}
+
+int validate_inputs(gapk_nr_batch b, const gapk_nr_inputs* in) {
+    if (!in || !in->d_y || !in->d_s_spec) {
+        set_error("inputs: d_y and d_s_spec are required");
+        return GAPK_EINVAL;
+    }
+    if (in->max_iterations < 0 || in->refine < 0 || in->refine > 8 ||
+        (in->policy < GAPK_POLICY_REFERENCE || in->policy > GAPK_POLICY_CLAMPED)) {
+        set_error("inputs: bad max_iterations / refine / policy");
+        return GAPK_EINVAL;
+    }
+    if (in->refine > 0 && !b->A64.p) {
+        set_error("inputs: refine > 0 needs a batch created with precision FP32");
+        return GAPK_EINVAL;
+    }
+    if (!(in->refine_below >= 0.0) || !(in->reuse_below >= 0.0)) {
+        set_error("inputs: refine_below and reuse_below must be >= 0");
+        return GAPK_EINVAL;
+    }
+    if (in->reuse_below > 0.0 && in->refine < 1) {
+        set_error("inputs: reuse_below > 0 needs refine >= 1");
+        return GAPK_EINVAL;
+    }
     return GAPK_OK;
 }
 
@@ -964,6 +986,230 @@ int gapk_nr_get_outputs(gapk_nr_batch b, const gapk_nr_outputs* out, void* strea
 }  // extern "C"
 
 // ===========================================================================================
+// Heterogeneous batches in one graph launch: every batch's whole solve (options, load, the
+// Newton loop in a device-side while node, optionally a retry loop for the scenarios that
+// did not converge, results out) is one branch of a single CUDA graph; the branches share no
+// edges, so the device runs them concurrently and one cudaGraphLaunch solves them all.
+// ===========================================================================================
+namespace gapk {
+namespace {
+
+template <typename T, int SW>
+struct InitOp {
+    static void run(gapk_nr_batch b, const gapk_nr_inputs* in, cudaStream_t st) {
+        k_init_ctrl<<<1, 32, 0, st>>>(b->dev, in->max_iterations, in->policy, in->tolerance,
+                                     in->refine_below, in->reuse_below);
+    }
+};
+template <typename T, int SW>
+struct RetryOp {
+    static void run(gapk_nr_batch b, const gapk_nr_inputs* in, int policy,
+                    cudaGraphConditionalHandle h, cudaStream_t st) {
+        PlanDev const& P = b->plan->dev;
+        k_retry_flags<SW><<<1, 1024, 0, st>>>(b->dev, policy, h);
+        dim3 g(blocks_for((long)P.n_bus * SW, 256), b->G);
+        k_retry_v<SW><<<g, 256, 0, st>>>(P, b->dev, reinterpret_cast<const double2*>(in->d_v_init),
+                                         in->d_u_pu, in->v_init_shared);
+    }
+};
+
+// Adds a while node after the capture's current dependencies on `cs` and captures the batch's
+// loop body into it on `body_stream`; the capture on `cs` then continues after the node.
+int add_loop(gapk_nr_batch b, cudaStream_t cs, cudaStream_t body_stream, unsigned dflt,
+             cudaGraphConditionalHandle* h_out) {
+    cudaStreamCaptureStatus stat;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    GAPK_CUDA_TRY(cudaStreamGetCaptureInfo(cs, &stat, nullptr, &g, &deps, &nd));
+    if (stat != cudaStreamCaptureStatusActive) {
+        set_error("mix graph: capture not active");
+        return GAPK_ECUDA;
+    }
+    cudaGraphConditionalHandle h;
+    GAPK_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, g, dflt, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    std::vector<cudaGraphNode_t> dv(nd);
+    for (size_t k = 0; k < nd; ++k) dv[k] = deps[k];
+    cudaGraphNode_t node;
+    GAPK_CUDA_TRY(cudaGraphAddNode(&node, g, dv.data(), dv.size(), &np));
+    GAPK_CUDA_TRY(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    cudaError_t e = cudaStreamBeginCaptureToGraph(body_stream, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        set_error(std::string("mix graph body capture: ") + cudaGetErrorString(e));
+        return GAPK_ECUDA;
+    }
+    dispatch_tsw<BodyOp>(b->precision, b->sw, b, body_stream, 1, h);
+    cudaGraph_t captured = nullptr;
+    GAPK_CUDA_TRY(cudaStreamEndCapture(body_stream, &captured));
+    *h_out = h;
+    return GAPK_OK;
+}
+
+}  // namespace
+}  // namespace gapk
+
+struct gapk_nr_mix_s {
+    std::vector<gapk_nr_batch> batches;
+    // the inputs / outputs the graph was built for, as bytes (the C structs are unnamed)
+    std::vector<unsigned char> in_bytes, out_bytes;
+    int retry = -2;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cs = nullptr, body = nullptr;
+    ~gapk_nr_mix_s() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (cs) cudaStreamDestroy(cs);
+        if (body) cudaStreamDestroy(body);
+    }
+    int build(const gapk_nr_inputs* ins, const gapk_nr_outputs* outs, int retry_policy) {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        if (!cs) GAPK_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        if (!body) GAPK_CUDA_TRY(cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking));
+        GAPK_CUDA_TRY(cudaGraphCreate(&graph, 0));
+        for (size_t i = 0; i < batches.size(); ++i) {
+            gapk_nr_batch b = batches[i];
+            b->cur_refine = ins[i].refine;
+            cudaError_t e = cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0,
+                                                          cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) {
+                set_error(std::string("mix graph capture: ") + cudaGetErrorString(e));
+                return GAPK_ECUDA;
+            }
+            int rc = GAPK_OK;
+            dispatch_tsw<InitOp>(b->precision, b->sw, b, &ins[i], cs);
+            dispatch_tsw<LoadOp>(b->precision, b->sw, b, &ins[i], cs);
+            cudaGraphConditionalHandle h{};
+            if (ins[i].max_iterations > 0) rc = add_loop(b, cs, body, 1, &h);
+            if (!rc && retry_policy >= 0 && ins[i].max_iterations > 0) {
+                cudaGraphConditionalHandle r{};
+                // the retry loop's condition starts false; k_retry_flags sets it
+                rc = add_loop_after(b, &ins[i], retry_policy, &r);
+            }
+            if (!rc) dispatch_tsw<StoreOp>(b->precision, b->sw, b, &outs[i], cs);
+            cudaGraph_t captured = nullptr;
+            cudaError_t e2 = cudaStreamEndCapture(cs, &captured);
+            if (rc) return rc;
+            if (e2 != cudaSuccess) {
+                set_error(std::string("mix graph capture end: ") + cudaGetErrorString(e2));
+                return GAPK_ECUDA;
+            }
+        }
+        GAPK_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
+        in_bytes.resize(batches.size() * sizeof(gapk_nr_inputs));
+        out_bytes.resize(batches.size() * sizeof(gapk_nr_outputs));
+        std::memcpy(in_bytes.data(), ins, in_bytes.size());
+        std::memcpy(out_bytes.data(), outs, out_bytes.size());
+        retry = retry_policy;
+        return GAPK_OK;
+    }
+    // retry: flags + start voltages (handle r, default 0), then a second loop on handle r
+    int add_loop_after(gapk_nr_batch b, const gapk_nr_inputs* in, int policy,
+                       cudaGraphConditionalHandle* r_out) {
+        cudaStreamCaptureStatus stat;
+        cudaGraph_t g = nullptr;
+        GAPK_CUDA_TRY(cudaStreamGetCaptureInfo(cs, &stat, nullptr, &g, nullptr, nullptr));
+        cudaGraphConditionalHandle r;
+        GAPK_CUDA_TRY(cudaGraphConditionalHandleCreate(&r, g, 0, cudaGraphCondAssignDefault));
+        dispatch_tsw<RetryOp>(b->precision, b->sw, b, in, policy, r, cs);
+        // the while node reads the condition k_retry_flags set
+        cudaStreamCaptureStatus stat2;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        GAPK_CUDA_TRY(cudaStreamGetCaptureInfo(cs, &stat2, nullptr, &g, &deps, &nd));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = r;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        std::vector<cudaGraphNode_t> dv(nd);
+    for (size_t k = 0; k < nd; ++k) dv[k] = deps[k];
+        cudaGraphNode_t node;
+        GAPK_CUDA_TRY(cudaGraphAddNode(&node, g, dv.data(), dv.size(), &np));
+        GAPK_CUDA_TRY(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+        cudaGraph_t bg = np.conditional.phGraph_out[0];
+        cudaError_t e = cudaStreamBeginCaptureToGraph(body, bg, nullptr, nullptr, 0,
+                                                      cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            set_error(std::string("mix graph retry body capture: ") + cudaGetErrorString(e));
+            return GAPK_ECUDA;
+        }
+        dispatch_tsw<BodyOp>(b->precision, b->sw, b, body, 1, r);
+        cudaGraph_t captured = nullptr;
+        GAPK_CUDA_TRY(cudaStreamEndCapture(body, &captured));
+        *r_out = r;
+        return GAPK_OK;
+    }
+};
+
+extern "C" {
+
+int gapk_nr_mix_create(int n, const gapk_nr_batch* batches, gapk_nr_mix* out) {
+    if (!out || n <= 0 || !batches) {
+        set_error("gapk_nr_mix_create: bad arguments");
+        return GAPK_EINVAL;
+    }
+    auto m = std::make_unique<gapk_nr_mix_s>();
+    for (int i = 0; i < n; ++i) {
+        if (!batches[i]) {
+            set_error("gapk_nr_mix_create: null batch");
+            return GAPK_EINVAL;
+        }
+        for (int j = 0; j < i; ++j)
+            if (batches[j] == batches[i]) {
+                set_error("gapk_nr_mix_create: a batch appears twice");
+                return GAPK_EINVAL;
+            }
+        m->batches.push_back(batches[i]);
+    }
+    *out = m.release();
+    return GAPK_OK;
+}
+
+int gapk_nr_mix_destroy(gapk_nr_mix m) {
+    delete m;
+    return GAPK_OK;
+}
+
+int gapk_nr_mix_solve(gapk_nr_mix m, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
+                      int retry_policy, void* stream) {
+    TraceRange tr("gapk_nr_mix_solve");
+    if (!m || !in || !out ||
+        (retry_policy != -1 &&
+         (retry_policy < GAPK_POLICY_REFERENCE || retry_policy > GAPK_POLICY_CLAMPED))) {
+        set_error("gapk_nr_mix_solve: bad arguments");
+        return GAPK_EINVAL;
+    }
+    const size_t n = m->batches.size();
+    for (size_t i = 0; i < n; ++i) {
+        int rc = validate_inputs(m->batches[i], &in[i]);
+        if (rc) return rc;
+    }
+    const bool same = m->exec && m->retry == retry_policy &&
+                      m->in_bytes.size() == n * sizeof(gapk_nr_inputs) &&
+                      std::memcmp(m->in_bytes.data(), in, m->in_bytes.size()) == 0 &&
+                      std::memcmp(m->out_bytes.data(), out, m->out_bytes.size()) == 0;
+    if (!same) {
+        int rc = m->build(in, out, retry_policy);
+        if (rc) return rc;
+    }
+    GAPK_CUDA_TRY(cudaGraphLaunch(m->exec, static_cast<cudaStream_t>(stream)));
+    return GAPK_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================================
 // General sparse LU (ILUSolver): complex a + jb handled as the 2x2 real block [a -b; b a], so
 // the Newton engine's analysis, level-scheduled factor, dense tail and solves are reused.
 // ===========================================================================================
@@ -1301,7 +1547,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
     if (rc) return rc;
     const int thr = 512;
     for (int it = 0; it < in->max_iterations; ++it) {
-        k_mismatch<1><<<blocks_for((long)n, 256), 256, 0, st>>>(P, D);
+        k_mismatch<1><<<mismatch_grid<1>(P, 1), 256, 0, st>>>(P, D);
         k_check<1><<<1, 1024, 0, st>>>(D, 0, cudaGraphConditionalHandle{});
         k_jfill<double, 1><<<blocks_for((long)h.n_a, 256), 256, 0, st>>>(P, D);
         k_factor<double, 1><<<1, thr, 0, st>>>(P, D);
@@ -1311,7 +1557,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
         }
         k_solve_fwd<double, 1><<<1, thr, 0, st>>>(P, D, D.rhs, 0);
         if (h.n_tail > 0)
-            k_dense_solve<double, 1><<<1, 256, N * sizeof(double), st>>>(P, D, D.dx, 0);
+            k_dense_solve<double, 1><<<1, 256, dense_solve_smem(P.n_tail, sizeof(double)), st>>>(P, D, D.dx, 0);
         k_solve_bwd<double, 1><<<1, thr, 0, st>>>(P, D, D.dx, 0);
         k_update<1><<<blocks_for((long)n, 256), 256, 0, st>>>(P, D);
         rc = check_launch();

@@ -154,41 +154,119 @@ __global__ void k_load(PlanDev P, BatchDev B, const double2* __restrict__ y_in,
 }
 
 // ---------------------------------------------------------------------------------------
+// in-graph control: solve options as kernel arguments, and the retry of unconverged lanes
+// ---------------------------------------------------------------------------------------
+// Loop control words and tolerances of one solve, written on the device (a graph that holds
+// several batches' loops sets each batch's options without host copies).
+__global__ void k_init_ctrl(BatchDev B, int max_iter, int policy, double tol, double refine_below,
+                            double reuse_below) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        B.ctrl[0] = 0;
+        B.ctrl[1] = max_iter;
+        B.ctrl[2] = 1;
+        B.ctrl[3] = policy;
+        B.ctrl[4] = 0;
+        B.tol[0] = tol;
+        B.tol[1] = refine_below;
+        B.tol[2] = reuse_below;
+    }
+}
+
+// Retry after the loop (one CTA): every scenario that ended at max_iterations or with a
+// non-finite mismatch starts again with the step policy `policy` (its other scenarios stay
+// done); the groups holding one iterate again, refactorising and refining.  Sets the retry
+// loop's condition to whether any scenario retries.
+template <int SW>
+__global__ void k_retry_flags(BatchDev B, int policy, cudaGraphConditionalHandle handle) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    const int total = B.n_groups * SW;
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        const bool again = q < B.n_scen && (B.status[q] == SC_MAXITER || B.status[q] == SC_NONFINITE);
+        if (again) {
+            B.state[q] = 0;
+            B.solving[q] = 1;
+            B.singular[q] = 0;
+            B.iters[q] = 0;
+            B.status[q] = SC_MAXITER;
+            B.mis_bits[q] = 0ull;
+            B.final_mis[q] = 0.0;
+            any = 1;  // benign race: every writer stores 1
+        }
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < B.n_groups; g += blockDim.x) {
+        int iv = 0;
+        for (int l = 0; l < SW; ++l) {
+            const int q = g * SW + l;
+            iv |= q < B.n_scen && B.state[q] == 0;
+        }
+        B.gsolve[g] = iv;
+        B.giter[g] = iv;
+        if (B.grefine) B.grefine[g] = 1;
+        if (B.gfactor) B.gfactor[g] = 1;
+    }
+    if (threadIdx.x == 0) {
+        B.ctrl[0] = 0;
+        B.ctrl[2] = any;
+        B.ctrl[3] = policy;
+        cudaGraphSetConditional(handle, any ? 1u : 0u);
+    }
+}
+
+// The retried scenarios' voltages back at their start (as k_load sets them).
+template <int SW>
+__global__ void k_retry_v(PlanDev P, BatchDev B, const double2* __restrict__ v_in,
+                          const double* __restrict__ u_pu, int v_shared) {
+    const int g = blockIdx.y;
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(tid / SW), lane = (int)(tid % SW);
+    const int q = g * SW + lane;
+    if (i >= P.n_bus || q >= B.n_scen || B.state[q] != 0) return;
+    double2 v;
+    if (v_in) {
+        v = v_in[(size_t)(v_shared ? 0 : q) * P.n_bus + i];
+    } else {
+        const int t = P.bus_type[i];
+        v = make_double2((t == BUS_PQ) ? 0.98 : (u_pu ? u_pu[i] : 1.0), 0.0);
+    }
+    B.V[((size_t)g * P.n_bus + i) * SW + lane] = v;
+}
+
+// ---------------------------------------------------------------------------------------
 // mismatch: fused Y*V SpMV, S = V conj(I), Delta, rhs, per-scenario max |Delta|
 // ---------------------------------------------------------------------------------------
+// Each CTA covers MM_TILES consecutive tiles of 256 / SW buses (x SW lanes); the per-scenario
+// maxima are reduced within the CTA (shuffles, then shared memory) before one atomicMax per
+// lane, so a group's scenarios see n / (MM_TILES * 256 / SW) atomics instead of one per warp
+// (same-address atomics serialise in L2).
+constexpr int MM_TILES = 4;
+
 template <int SW>
 __global__ void __launch_bounds__(256, 8) k_mismatch(PlanDev P, BatchDev B) {
     const int g = blockIdx.y;
     if (!B.giter[g]) return;
     const int n = P.n_bus;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = tid / SW, lane = tid % SW;
+    const int lane = threadIdx.x % SW;
+    const double2* Vg = B.V + (size_t)g * n * SW;
+    const double2* Yg = B.y_shared ? B.Y : B.Y + (size_t)g * P.nnz_y * SW;
+    const int ys = B.y_shared ? 0 : 1;  // Y value of entry p at Yg[p * (ys ? SW : 1) + ys * lane]
     double m = 0.0;
-    if (i < n) {
-        const double2* Vg = B.V + (size_t)g * n * SW;
+#pragma unroll 1
+    for (int tile = 0; tile < MM_TILES; ++tile) {
+        const int i = ((blockIdx.x * MM_TILES + tile) * blockDim.x + threadIdx.x) / SW;
+        if (i >= n) break;
         const int pb = P.y_row_ptr[i], pe = P.y_row_ptr[i + 1];
         double ir = 0.0, ii = 0.0;
-        if (B.y_shared) {
 #pragma unroll 4
-            for (int p = pb; p < pe; ++p) {
-                const double2 y = B.Y[p];
-                const double2 v = Vg[(size_t)P.y_col[p] * SW + lane];
-                ir = fma(y.x, v.x, ir);
-                ir = fma(-y.y, v.y, ir);
-                ii = fma(y.x, v.y, ii);
-                ii = fma(y.y, v.x, ii);
-            }
-        } else {
-            const double2* Yg = B.Y + (size_t)g * P.nnz_y * SW;
-#pragma unroll 4
-            for (int p = pb; p < pe; ++p) {
-                const double2 y = Yg[(size_t)p * SW + lane];
-                const double2 v = Vg[(size_t)P.y_col[p] * SW + lane];
-                ir = fma(y.x, v.x, ir);
-                ir = fma(-y.y, v.y, ir);
-                ii = fma(y.x, v.y, ii);
-                ii = fma(y.y, v.x, ii);
-            }
+        for (int p = pb; p < pe; ++p) {
+            const double2 y = ys ? Yg[(size_t)p * SW + lane] : Yg[p];
+            const double2 v = Vg[(size_t)P.y_col[p] * SW + lane];
+            ir = fma(y.x, v.x, ir);
+            ir = fma(-y.y, v.y, ir);
+            ii = fma(y.x, v.y, ii);
+            ii = fma(y.y, v.x, ii);
         }
         const size_t o = ((size_t)g * n + i) * SW + lane;
         const double2 vi = Vg[(size_t)i * SW + lane];
@@ -202,14 +280,28 @@ __global__ void __launch_bounds__(256, 8) k_mismatch(PlanDev P, BatchDev B) {
             const double dq = (t == BUS_PQ) ? s.y - sp.y : 0.0;
             const int node = P.node_of_bus[i];
             B.rhs[((size_t)g * P.nb + node) * SW + lane] = make_double2(-dp, -dq);
-            m = nmax(fabs(dp), fabs(dq));
+            m = nmax(m, nmax(fabs(dp), fabs(dq)));
         }
     }
 #pragma unroll
     for (int off = SW; off < 32; off <<= 1) m = nmax(m, __shfl_xor_sync(0xffffffffu, m, off));
-    if ((threadIdx.x & 31) < SW && m != 0.0) {
-        atomicMax(&B.mis_bits[g * SW + lane], (unsigned long long)__double_as_longlong(m));
+    __shared__ double red[8][8];  // [warp][lane] (blockDim 256, SW <= 8)
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) < SW) red[w][lane] = m;
+    __syncthreads();
+    if (threadIdx.x < SW) {
+        double r = red[0][threadIdx.x];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) r = nmax(r, red[k][threadIdx.x]);
+        if (r != 0.0)
+            atomicMax(&B.mis_bits[g * SW + threadIdx.x], (unsigned long long)__double_as_longlong(r));
     }
+}
+
+// Grid of k_mismatch for G lane groups.
+template <int SW>
+inline dim3 mismatch_grid(PlanDev const& P, int G) {
+    const long per = (long)MM_TILES * 256;
+    return dim3((unsigned)(((long)P.n_bus * SW + per - 1) / per), (unsigned)G);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -959,11 +1051,53 @@ void launch_dense_lu_split(int grid, cudaStream_t st, BatchDev const& B, int N) 
 }
 
 // Forward (unit L) then backward (U) substitution on one scenario's tail vector, blocked by
-// 32 rows: all warps form the dot products with the already-solved part, warp 0 solves the
-// 32x32 triangle with shuffles.
+// 32 rows.  Per block, the dot products of its rows with the solved part stream the factor:
+// warp w takes rows w, w + 8, w + 16, w + 24 of the block together, each lane reading one
+// 4-element vector per row per step (128 columns per warp-wide load), so every thread keeps
+// four vector loads in flight; the block's 32 x 32 triangle is staged in shared memory by the
+// whole CTA (one vector per thread) at the same time, and warp 0 then solves it with shuffles.
+// At <= 36 registers, seven CTAs fit on an SM, so a 1024-scenario batch runs in one wave.  y
+// lives in shared memory, ld = dense_ld(N) entries, zero beyond N (the factor's padding
+// columns hold no values and are masked).
+template <typename T>
+__device__ __forceinline__ void dense_dot4(const T* __restrict__ A, int ld, int r0, int wid,
+                                           int ln, int cb, int ce, int N, const T* y, T acc[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) acc[i] = T(0);
+#pragma unroll 1
+    for (int c = cb + 4 * ln; c < ce; c += 128) {
+        const V4<T> yv = ld4(y + c);
+        V4<T> a[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int row = r0 + wid + 8 * i;
+            a[i] = row < N ? ld4(A + (size_t)row * ld + c) : V4<T>{{T(0), T(0), T(0), T(0)}};
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int t = 0; t < 4; ++t) acc[i] = fma(c + t < N ? a[i].v[t] : T(0), yv.v[t], acc[i]);
+    }
+}
+
+// The 32 x 32 diagonal block at (r0, r0) into tri[32][33], one 4-vector per thread of the
+// first 256 (a vector that starts inside the padded row ends inside it, ld % 8 == 0).
+template <typename T>
+__device__ __forceinline__ void dense_stage_tri(const T* __restrict__ A, int ld, int r0, int N,
+                                                T (*tri)[33]) {
+    const int t = threadIdx.x;
+    if (t < 256) {
+        const int r = t >> 3, c = (t & 7) * 4;
+        const V4<T> v = r0 + r < N && r0 + c < ld ? ld4(A + (size_t)(r0 + r) * ld + r0 + c)
+                                                 : V4<T>{{T(0), T(0), T(0), T(0)}};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) tri[r][c + k] = v.v[k];
+    }
+}
+
 template <typename T, int SW>
-__global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, double2* out,
-                                                     int accumulate) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 7 : 4) k_dense_solve(PlanDev P, BatchDev B, double2* out,
+                                                        int accumulate) {
     const int q = blockIdx.x;
     if (q >= B.n_scen || !B.solving[q]) return;
     const int g = q / SW, lane = q % SW;
@@ -973,22 +1107,31 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
     Vec2<T>* X = reinterpret_cast<Vec2<T>*>(B.X) + (size_t)g * P.nb * SW;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* y = reinterpret_cast<T*>(smraw);
-    const int tid = threadIdx.x, wid = tid >> 5, ln = tid & 31, nw = blockDim.x >> 5;
-    for (int i = tid; i < P.n_tail; i += blockDim.x) {
-        const Vec2<T> v = ldv(X + (size_t)(P.ns + i) * SW + lane);
+    __shared__ T tri[32][33];
+    const int tid = threadIdx.x, wid = tid >> 5, ln = tid & 31;
+    for (int i = tid; i < ld / 2; i += blockDim.x) {
+        const Vec2<T> v = i < P.n_tail ? ldv(X + (size_t)(P.ns + i) * SW + lane) : Vec2<T>{T(0), T(0)};
         y[2 * i] = v.x;
         y[2 * i + 1] = v.y;
     }
     __syncthreads();
+    // L y = b, unit lower
     for (int r0 = 0; r0 < N; r0 += 32) {
-        for (int rr = wid; rr < 32; rr += nw) {
-            const int row = r0 + rr;
-            if (row >= N) continue;
-            T acc = T(0);
-            for (int c = ln; c < r0; c += 32) acc = fma(A[(size_t)row * ld + c], y[c], acc);
+        dense_stage_tri<T>(A, ld, r0, N, tri);
+        if (r0 > 0) {
+            T acc[4];
+            // blockDim is 256: 8 warps x 4 rows = the 32 rows of the block
+            dense_dot4<T>(A, ld, r0, wid, ln, 0, r0, N, y, acc);
 #pragma unroll
-            for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-            if (ln == 0) y[row] -= acc;
+            for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                for (int off = 16; off; off >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+            }
+            if (ln == 0) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (r0 + wid + 8 * i < N) y[r0 + wid + 8 * i] -= acc[i];
+            }
         }
         __syncthreads();
         if (wid == 0) {
@@ -996,33 +1139,41 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
             T v = row < N ? y[row] : T(0);
             for (int j = 0; j < 32; ++j) {
                 const T vj = __shfl_sync(0xffffffffu, v, j);
-                if (ln > j && row < N && r0 + j < N) v = fma(-A[(size_t)row * ld + r0 + j], vj, v);
+                if (ln > j && row < N && r0 + j < N) v = fma(-tri[ln][j], vj, v);
             }
             if (row < N) y[row] = v;
         }
         __syncthreads();
     }
+    // U x = y
     const int last = ((N - 1) / 32) * 32;
     for (int r0 = last; r0 >= 0; r0 -= 32) {
         const int r1 = min(r0 + 32, N);
-        for (int rr = wid; rr < 32; rr += nw) {
-            const int row = r0 + rr;
-            if (row >= N) continue;
-            T acc = T(0);
-            for (int c = r1 + ln; c < N; c += 32) acc = fma(A[(size_t)row * ld + c], y[c], acc);
+        dense_stage_tri<T>(A, ld, r0, N, tri);
+        if (r1 < N) {
+            T acc[4];
+            dense_dot4<T>(A, ld, r0, wid, ln, r1, ld, N, y, acc);
 #pragma unroll
-            for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-            if (ln == 0) y[row] -= acc;
+            for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                for (int off = 16; off; off >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+            }
+            if (ln == 0) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (r0 + wid + 8 * i < N) y[r0 + wid + 8 * i] -= acc[i];
+            }
         }
         __syncthreads();
         if (wid == 0) {
             const int row = r0 + ln;
             T v = row < N ? y[row] : T(0);
             for (int j = 31; j >= 0; --j) {
-                if (r0 + j >= N) continue;
-                if (ln == j) v = v / A[(size_t)row * ld + row];
-                const T vj = __shfl_sync(0xffffffffu, v, j);
-                if (ln < j && row < N) v = fma(-A[(size_t)row * ld + r0 + j], vj, v);
+                if (r0 + j < N) {
+                    if (ln == j) v = v / tri[j][j];
+                    const T vj = __shfl_sync(0xffffffffu, v, j);
+                    if (ln < j && row < N) v = fma(-tri[ln][j], vj, v);
+                }
             }
             if (row < N) y[row] = v;
         }
@@ -1040,6 +1191,11 @@ __global__ void __launch_bounds__(256) k_dense_solve(PlanDev P, BatchDev B, doub
             *o = make_double2((double)y[2 * i], (double)y[2 * i + 1]);
         }
     }
+}
+
+// Dynamic shared memory of k_dense_solve / k_dense_solve_t: the tail vector, padded to ld.
+__host__ __forceinline__ size_t dense_solve_smem(int n_tail, size_t esz) {
+    return (size_t)dense_ld(2 * n_tail) * esz;
 }
 
 // ---------------------------------------------------------------------------------------

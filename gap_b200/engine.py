@@ -489,6 +489,63 @@ class NRBatch:
             pass
 
 
+class NRMix:
+    """Batches of any plans solved together by ONE graph launch (gapk_nr_mix_*): each batch's
+    whole solve is one branch of a single CUDA graph, the branches run concurrently, and with
+    `retry` the scenarios that end unconverged restart from their start vector under that step
+    policy inside the same launch.  The graph is built on the first solve and reused while the
+    input tensors and options stay the same; results land in the same tensors every time
+    (self.results)."""
+
+    def __init__(self, batches):
+        require_cuda()
+        self.batches = list(batches)
+        arr = (C.c_void_p * len(self.batches))(*[b._h.value for b in self.batches])
+        h = C.c_void_p()
+        N.check(N.lib().gapk_nr_mix_create(len(self.batches), arr, C.byref(h)))
+        self._h = h
+        torch = _torch()
+        self.results = []
+        for b in self.batches:
+            n = b.plan.info["n_bus"]
+            self.results.append(NRResult(
+                torch.empty((b.n_scen, n), dtype=torch.complex128, device="cuda"),
+                torch.empty(b.n_scen, dtype=torch.int32, device="cuda"),
+                torch.empty(b.n_scen, dtype=torch.int32, device="cuda"),
+                torch.empty(b.n_scen, dtype=torch.float64, device="cuda")))
+
+    def solve(self, ys, s_specs, v_inits=None, u_pus=None, tol=1e-8, max_iter=20,
+              policy="newton", refine=0, refine_below=0.0, reuse_below=0.0, retry=None,
+              stream=None):
+        """ys / s_specs / v_inits / u_pus: one entry per batch, as NRBatch.solve takes them
+        (keep the same tensors between calls to reuse the graph); retry: None or a step policy
+        name.  Returns self.results (NRResult per batch), written asynchronously on the
+        stream."""
+        nb = len(self.batches)
+        v_inits = v_inits if v_inits is not None else [None] * nb
+        u_pus = u_pus if u_pus is not None else [None] * nb
+        ins = (N.Inputs * nb)(*[b._inputs(y, s, v, u, tol, max_iter, policy, refine,
+                                          refine_below, reuse_below)
+                                for b, y, s, v, u in zip(self.batches, ys, s_specs, v_inits,
+                                                         u_pus)])
+        outs = (N.Outputs * nb)(*[N.Outputs(_dptr(r.v), _dptr(r.iterations), _dptr(r.status),
+                                            _dptr(r.final_mismatch)) for r in self.results])
+        pol = -1 if retry is None else {"reference": N.POLICY_REFERENCE,
+                                        "newton": N.POLICY_NEWTON,
+                                        "clamped": N.POLICY_CLAMPED}[retry]
+        self._keep = (ys, s_specs, v_inits, u_pus)
+        N.check(N.lib().gapk_nr_mix_solve(self._h, ins, outs, pol, _stream_ptr(stream)))
+        return self.results
+
+    def __del__(self):
+        try:
+            if self._h:
+                N.lib().gapk_nr_mix_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
 class HostPipeline:
     """Batched solves from and to host memory with the copies overlapped: the scenarios are
     split into `chunks` contiguous parts (multiples of the lane count), each with its own

@@ -26,7 +26,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
-from .engine import (NRBatch, NRPlan, NRResult, YbusDelta, YbusPlan, branch_params,
+from .engine import (NRBatch, NRMix, NRPlan, NRResult, YbusDelta, YbusPlan, branch_params,
                      shunt_params)
 from .network import Network
 
@@ -238,6 +238,62 @@ def timed_concurrent(studies, steps=3, warmup=1, **kw):
     e0.record()
     for _ in range(steps):
         solve_concurrent(studies, **kw)
+    e1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    conv = sum(int((st.result.status == 0).sum().item()) for st in studies)
+    return e0.elapsed_time(e1) / steps, conv, wall / steps
+
+
+# ----------------------------------------------------------------------------------------
+# one launch for the whole mix
+# ----------------------------------------------------------------------------------------
+
+_MIXES: "weakref.WeakValueDictionary" = weakref.WeakValueDictionary()
+
+
+class _MixHolder:
+    def __init__(self, mix):
+        self.mix = mix
+
+
+def solve_mixed(studies, tol=1e-8, max_iter=20, policy="newton", refine=1, refine_below=0.0,
+                reuse_below=0.0, retry="clamped", stream=None):
+    """Every study solved by ONE graph launch (engine.NRMix over the studies' batches): each
+    study's solve is a branch of the graph; with `retry`, scenarios that end unconverged restart
+    from their start vector under that step policy inside the same launch.  Results land in
+    `study.result` (the same tensors on every call; asynchronous on the stream)."""
+    for st in studies:
+        st.make_batch()
+    key = tuple(id(st.batch) for st in studies)
+    holder = _MIXES.get(key)
+    if holder is None:
+        holder = _MixHolder(NRMix([st.batch for st in studies]))
+        _MIXES[key] = holder
+        for st in studies:
+            st.info["_mix"] = holder  # keeps the mix alive as long as its studies
+    res = holder.mix.solve([st.y for st in studies], [st.s_spec for st in studies],
+                           [st.v0 for st in studies], tol=tol, max_iter=max_iter, policy=policy,
+                           refine=refine, refine_below=refine_below, reuse_below=reuse_below,
+                           retry=retry, stream=stream)
+    for st, r in zip(studies, res):
+        st.result = r
+    return res
+
+
+def timed_mixed(studies, steps=3, warmup=1, **kw):
+    """Device time (ms, CUDA events) of `steps` one-launch solves of the whole mix after
+    `warmup` solves, the converged count of the last solve and the host wall time per step."""
+    torch = _torch()
+    for _ in range(warmup):
+        solve_mixed(studies, **kw)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record()
+    for _ in range(steps):
+        solve_mixed(studies, **kw)
     e1.record()
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0

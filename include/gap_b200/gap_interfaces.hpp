@@ -12,6 +12,7 @@
 //   include/gap/solver/lu_solver_interface.h:12-48        (ILUSolver)
 //   include/gap/solver/powerflow_interface.h:13-108       (PowerFlowConfig, IterationState,
 //                                                           PowerFlowResult, IPowerFlowSolver)
+//   include/gap/io/io_interface.h:8-44                    (IIOModule)
 // Only layout-relevant declarations are repeated (no inline helpers, no GPU mirror structs).
 // tests/test_gpu_plugins.py loads the plugins from a driver compiled against the reference's
 // own headers, which checks that the two agree.
@@ -160,5 +161,16 @@ class IPowerFlowSolver {
     virtual void clear_iteration_states() {}
 };
 }  // namespace solver
+
+namespace io {
+class IIOModule {
+  public:
+    virtual ~IIOModule() = default;
+    virtual NetworkData read_network_data(std::string const& filename) = 0;
+    virtual void write_results(std::string const& filename, ComplexVector const& bus_voltages,
+                               bool converged, int iterations) = 0;
+    virtual bool validate_input_format(std::string const& filename) = 0;
+};
+}  // namespace io
 
 }  // namespace gap

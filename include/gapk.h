@@ -261,6 +261,24 @@ typedef struct {
 int gapk_nr_solve(gapk_nr_batch b, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
                   void* stream);
 
+/* ==== Heterogeneous batches in one launch (no reference counterpart) ======================
+ * Batches of different plans (load scenarios of one grid, its N-1 contingencies sharing that
+ * grid's plan, independent grids of any size) solved by ONE cudaGraphLaunch: each batch's whole
+ * solve -- its options, its inputs loaded, its Newton loop as a device-side while node, results
+ * written -- is one branch of a single graph, and the branches run concurrently.  Per-scenario
+ * status words as gapk_nr_solve's.  With retry_policy >= 0 (a GAPK_POLICY_*), the scenarios
+ * that end at max_iterations or with a non-finite mismatch restart from their start vector
+ * under that policy, inside the same launch (a second while node per branch whose condition
+ * the device sets); their iteration count is then the retry's.  The graph is built on the first
+ * call and rebuilt only when an input/output pointer or option changes; a batch belongs to at
+ * most one mix at a time and is not solved on its own while the mix runs. */
+typedef struct gapk_nr_mix_s* gapk_nr_mix;
+int gapk_nr_mix_create(int n_batches, const gapk_nr_batch* batches, gapk_nr_mix* out);
+int gapk_nr_mix_destroy(gapk_nr_mix m);
+/* in[i] / out[i] for batch i (as for gapk_nr_solve); asynchronous on `stream`. */
+int gapk_nr_mix_solve(gapk_nr_mix m, const gapk_nr_inputs* in, const gapk_nr_outputs* out,
+                      int retry_policy, void* stream);
+
 /* ==== Stepping, for iteration-state capture ===============================================
  * IPowerFlowSolver::enable_state_capture / get_iteration_states
  * (include/gap/solver/powerflow_interface.h:28-35,83-107; recorded per iteration by

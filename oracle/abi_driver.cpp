@@ -7,6 +7,12 @@
 // compares them with the reference CPU backends through the reference's own interfaces.
 //
 //   abi_driver <plugin_dir> <network.txt>
+//   abi_driver --io <plugin_dir> <pgm_input.json>
+//
+// --io loads libgap_io_pgm.so (create_pgm_io_module) as an IIOModule and prints the NetworkData
+// it reads ("bus id u_rated type u_pu", "br id from to status r1 x1 g1 b1 k theta i_n sn",
+// "app id node status type p_specified q_specified g1 b1 u_ref"), so the reader is checked
+// through the reference's own NetworkData layout.
 //
 // network.txt: "n" then n lines "id u_rated type u_pu p q"; "m" then m lines
 // "id from to status r1 x1 g1 b1 k theta"; "a" then a lines "id node status type p q g1 b1";
@@ -18,6 +24,9 @@
 #include <fstream>
 #include <iostream>
 
+#include <iomanip>
+
+#include "gap/io/io_interface.h"
 #include "src/admittance/cpu/cpu_admittance_matrix.cpp"
 #include "src/solver/lu/cpu/cpu_lu_solver.cpp"
 #include "src/solver/powerflow/cpu/cpu_newton_raphson.cpp"
@@ -39,10 +48,34 @@ static F load(std::string const& dir, const char* lib, const char* sym) {
     return reinterpret_cast<F>(f);
 }
 
+static int read_with_io_module(std::string const& dir, std::string const& file) {
+    using CI = io::IIOModule* (*)();
+    std::unique_ptr<io::IIOModule> m(load<CI>(dir, "libgap_io_pgm.so", "create_pgm_io_module")());
+    std::cout << std::setprecision(17) << "valid " << m->validate_input_format(file) << "\n";
+    NetworkData net = m->read_network_data(file);
+    std::cout << "counts " << net.num_buses << " " << net.num_branches << " "
+              << net.num_appliances << " " << net.buses.size() << " " << net.branches.size()
+              << " " << net.appliances.size() << "\n";
+    for (auto const& b : net.buses)
+        std::cout << "bus " << b.id << " " << b.u_rated << " " << static_cast<int>(b.bus_type)
+                  << " " << b.u_pu << "\n";
+    for (auto const& b : net.branches)
+        std::cout << "br " << b.id << " " << b.from_bus << " " << b.to_bus << " "
+                  << static_cast<int>(b.status) << " " << b.r1 << " " << b.x1 << " " << b.g1
+                  << " " << b.b1 << " " << b.k << " " << b.theta << " " << b.i_n << " " << b.sn
+                  << "\n";
+    for (auto const& a : net.appliances)
+        std::cout << "app " << a.id << " " << a.node << " " << static_cast<int>(a.status) << " "
+                  << static_cast<int>(a.type) << " " << a.p_specified << " " << a.q_specified
+                  << " " << a.g1 << " " << a.b1 << " " << a.u_ref << "\n";
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 3) return 2;
     gap::logging::Logger::getInstance().configure(gap::logging::LogLevel::OFF,
                                                   gap::logging::LogOutput::NONE);
+    if (std::string(argv[1]) == "--io") return argc < 4 ? 2 : read_with_io_module(argv[2], argv[3]);
     std::ifstream in(argv[2]);
     NetworkData net;
     int n, m, a;

@@ -96,7 +96,7 @@ def test_adjoint_at_transmission_scale():
     assert _rel_ok(x.grad.cpu().numpy(), dx_tot) < REL
 
 
-H_PQ, H_RX = 4e-3, 5e-2
+H_PQ, H_R, H_X = 4e-3, 5e-2, 2e-2
 UNIT = (1, -1, 2, -2, 4, -4)
 
 
@@ -106,8 +106,9 @@ def _fd_check(net, s, kw, n_pq, n_rx, seed):
     and buses) and n_rx r and n_rx x values (random branches, shared by every scenario).
 
     The difference quotient is extrapolated twice (Richardson), D = (64 D(h) - 20 D(2h) +
-    D(4h)) / 45 with D(h) = (L(+h) - L(-h)) / 2h, h = 4e-3 pu for P / Q and 5e-2 of the value
-    for r / x: its truncation error is O(h^6).  The perturbed solves run a fixed 12 Newton
+    D(4h)) / 45 with D(h) = (L(+h) - L(-h)) / 2h, h = 4e-3 pu for P / Q and 5e-2 (r), 2e-2
+    (x) of the value for the branch parameters: its truncation error is O(h^6) (x, which sets
+    |z|, is the more nonlinear of the two).  The perturbed solves run a fixed 12 Newton
     iterations (tolerance 0), which takes every scenario to its rounding floor.  The steps are
     large because the loss of a converged solve carries rounding noise that differs from solve
     to solve (the Newton fixed point moves with the last bits of the mismatch, times the
@@ -150,14 +151,16 @@ def _fd_check(net, s, kw, n_pq, n_rx, seed):
     brs = ([("r", int(rng.choice(inservice))) for _ in range(n_rx)] +
            [("x", int(rng.choice(inservice))) for _ in range(n_rx)])
 
+    def step(kind):
+        return {"p": H_PQ, "q": H_PQ, "r": H_R, "x": H_X}[kind]
+
     def steps(kind):
-        h = H_PQ if kind in ("p", "q") else H_RX
-        return [u * h for u in UNIT] + [1e-6, -1e-6]
+        return [u * step(kind) for u in UNIT] + [1e-6, -1e-6]
 
     fd, fd_plain, ad, kinds = [], [], [], []
 
     def record(kind, L8, scale, grad):
-        H = H_PQ if kind in ("p", "q") else H_RX
+        H = step(kind)
         d1 = (L8[0] - L8[1]) / (2 * H * scale)
         d2 = (L8[2] - L8[3]) / (4 * H * scale)
         d4 = (L8[4] - L8[5]) / (8 * H * scale)
