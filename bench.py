@@ -213,6 +213,9 @@ def algorithmic_bytes(kernel, info, n_scen, esz):
         return S * 2 * (ns_slots - T * T) * blk
     if kernel in ("solve_fwd", "solve_bwd"):
         return S * (nnzl * blk + nb * 16 * 2)
+    if kernel == "residual":
+        # FP64 Jacobian blocks, the correction and the right-hand side read, the residual written
+        return S * (info["n_a_blocks"] * 32 + nb * 16 * 3)
     if kernel == "update":
         return S * (n * 32 + nb * 16)
     return 0
@@ -378,7 +381,7 @@ def run_ours(args, rank, world, device):
             "source": "per-panel stamps of one CTA (one scenario), median over scenarios; "
                       "CTAs run 2 per SM in 3.5 waves"}
     per_iter = {"mismatch": 1, "jacobian": 1, "factor_sparse": 1, "schur": 1, "dense_lu": 1,
-                "solve_fwd": 2, "dense_solve": 2, "solve_bwd": 2, "update": 1}
+                "solve_fwd": 2, "dense_solve": 2, "solve_bwd": 2, "update": 1, "residual": 1}
     if info["n_tail"] == 0:
         for k in ("schur", "dense_lu", "dense_solve"):
             per_iter[k] = 0
@@ -398,6 +401,14 @@ def run_ours(args, rank, world, device):
     # FP32 FMA rate of the dense LU (2/3 N^3 flops per scenario), for the kernels that compute
     fma_tflops = (N_SCEN * 2.0 / 3.0 * (2 * info["n_tail"]) ** 3 / (kt["dense_lu"] / 1e3) / 1e12
                   if info["n_tail"] and dom == "dense_lu" else None)
+    # every kernel of the loop against the same HBM roof (algorithmic bytes / CUDA-event time)
+    kernel_roofline = {}
+    for k in kt:
+        b = algorithmic_bytes(k, info, N_SCEN, esz)
+        if b and kt[k] > 0:
+            gbs = b / (kt[k] / 1e3) / 1e9
+            kernel_roofline[k] = {"ms": kt[k], "algorithmic_bytes": b, "achieved_gbs": gbs,
+                                  "frac": gbs / hbm}
     launches_per_iter = 6 + 3 * 2 + 1 + 1 if info["n_tail"] else 4 + 2 * 2 + 1 + 1
     gpu_launches = args.steps * (2 + loops * launches_per_iter)
 
@@ -451,6 +462,7 @@ def run_ours(args, rank, world, device):
                          "fp32_fma_tflops": fma_tflops,
                          "launch_ms": kt[dom], "peak_source": "measured" if peaks else "fallback"},
             "kernel_ms": kt, "kernel_share_ms_per_iter": share, "lu_levels": lu_levels,
+            "kernel_roofline": kernel_roofline,
             "plain_fp64_single": plain,
             "batched_over_plain_fp64": value / plain["value"] if plain["value"] else None,
             "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": gpu_launches,

@@ -344,6 +344,9 @@ struct KernelOp {
                 break;
             case 7: k_solve_bwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.dx, 0); break;
             case 8: k_update<SW><<<dim3(blocks_for((long)P.n_bus * SW, 256), G), 256, 0, st>>>(P, B); break;
+            case 9:
+                if (B.A64) k_residual<SW><<<dim3(blocks_for((long)P.nb * SW, 256), G), 256, 0, st>>>(P, B);
+                break;
         }
     }
 };
@@ -860,7 +863,7 @@ int gapk_nr_stage_factor(gapk_nr_batch b, void* s) { return stage(b, 2, s); }
 int gapk_nr_stage_solve(gapk_nr_batch b, void* s) { return stage(b, 3, s); }
 
 int gapk_nr_stage_kernel(gapk_nr_batch b, int kernel, void* stream) {
-    if (!b || kernel < 0 || kernel > 8) {
+    if (!b || kernel < 0 || kernel > 9) {
         set_error("gapk_nr_stage_kernel: bad arguments");
         return GAPK_EINVAL;
     }

@@ -1488,12 +1488,19 @@ __global__ void __launch_bounds__(256, 8) k_update(PlanDev P, BatchDev B) {
             v = make_double2(vmn * cs, vmn * sn);
         }
     } else {
-        double vm = hypot(v.x, v.y);
-        const double va = atan2(v.y, v.x) + d.x;
-        if (pq) vm += d.y;
+        // Newton step in polar form, |V| e^{j theta} -> (|V| + d|V|) e^{j (theta + dtheta)}:
+        // V rotated by dtheta and scaled by (|V| + d|V|) / |V|, one sincos of the (small)
+        // correction instead of atan2 and a sincos of the full angle
+        const double vm = hypot(v.x, v.y);
         double sn, cs;
-        sincos(va, &sn, &cs);
-        v = make_double2(vm * cs, vm * sn);
+        sincos(d.x, &sn, &cs);
+        if (vm > 0.0) {
+            const double sc = pq ? (vm + d.y) / vm : 1.0;
+            v = make_double2(sc * fma(v.x, cs, -v.y * sn), sc * fma(v.x, sn, v.y * cs));
+        } else {
+            const double m = pq ? d.y : 0.0;  // from V = 0 the angle is the correction's
+            v = make_double2(m * cs, m * sn);
+        }
     }
     B.V[o] = v;
 }

@@ -400,7 +400,7 @@ class NRBatch:
         N.check(getattr(N.lib(), fn)(self._h, _stream_ptr(stream)))
 
     KERNELS = ("mismatch", "jacobian", "factor_sparse", "schur", "dense_lu", "solve_fwd",
-               "dense_solve", "solve_bwd", "update")
+               "dense_solve", "solve_bwd", "update", "residual")
 
     def kernel(self, name, stream=None):
         """Launch one kernel of the loop body (timing / profiling)."""

@@ -383,6 +383,7 @@ int gapk_nr_stage_solve(gapk_nr_batch b, void* stream);
 /* One kernel of the loop body, for per-kernel timing and profiling:
  *   0 mismatch  1 jacobian fill  2 sparse factor  3 Schur gather  4 dense LU
  *   5 sparse forward solve  6 dense solve  7 sparse backward solve  8 update
+ *   9 refinement residual (FP32 batches)
  * Kernels 3, 4 and 6 do nothing when the plan has no dense tail. */
 int gapk_nr_stage_kernel(gapk_nr_batch b, int kernel, void* stream);
 /* Newton correction of the last stage_solve, [n_scen][n_vars] doubles in the reference's
