@@ -271,7 +271,8 @@ def run_ours(args, rank, world, device):
     plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
     plan_s = time.perf_counter() - t0
     info = plan.info
-    batch = NRBatch(plan, N_SCEN, use_graph=not args.host_loop, **workloads.batch_kwargs())
+    batch = NRBatch(plan, N_SCEN, use_graph=not args.host_loop, dense_tc=args.dense_tc,
+                    **workloads.batch_kwargs())
     s_dev = torch.as_tensor(s_np, device="cuda")
     v_dev = torch.as_tensor(v_np, device="cuda")
 
@@ -448,6 +449,8 @@ def run_ours(args, rank, world, device):
             "data": "synthetic (seeded generator, no external dataset)",
             "config": config({"parallelism": f"scenario shards x{world}",
                               "newton_loop": "host" if args.host_loop else "cuda graph",
+                              "dense_lu": "tensor cores (device batch)" if args.dense_tc
+                                          else "cuda-core fma",
                               "converged_per_step": conv_all,
                               "max_iterations_run": int(iters.max()), "plan_seconds": plan_s}),
             "e2e": {"value": conv_e2e * args.steps / (e2e_ms / 1e3), "unit": "solves/s",
@@ -799,6 +802,9 @@ def main():
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Newton loop from the host instead of one CUDA graph with a "
                          "conditional node (same kernels and work; lets ncu see every launch)")
+    ap.add_argument("--dense-tc", action="store_true",
+                    help="device-resident batch only: the dense-tail LU with its trailing update "
+                         "on the tensor cores (k_dense_lu_tc) instead of CUDA-core FMA")
     args = ap.parse_args()
     N_SCEN = args.scenarios
     rank = int(os.environ.get("RANK", "0"))

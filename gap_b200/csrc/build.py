@@ -46,7 +46,7 @@ def _run(cmd):
 
 
 CORE_SOURCES = ["symbolic.cpp", "nr.cu", "ybus.cu"]
-HEADERS = ["internal.h", "blocks.cuh", "nr_kernels.cuh"]
+HEADERS = ["internal.h", "blocks.cuh", "nr_kernels.cuh", "dense_lu_tc.cuh"]
 
 
 def build(verbose: bool = False, force: bool = False) -> str:

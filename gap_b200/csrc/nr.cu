@@ -159,6 +159,7 @@ struct gapk_nr_batch_s {
     int dense_w = 0;          // panel width of the one-CTA-per-scenario dense LU (0: not used)
     size_t dense_smem = 0;    // its dynamic shared memory
     bool dense_split = false; // factorise the tail with the split kernels
+    bool dense_tc = false;    // the one-CTA-per-scenario LU with the tensor-core trailing update
     BatchDev dev{};
     // graph cache
     cudaGraph_t graph = nullptr;
@@ -198,7 +199,7 @@ void launch_factor(gapk_nr_batch b, cudaStream_t st) {
         if (b->dense_split)
             launch_dense_lu_split<T>(b->G * SW, st, B, 2 * P.n_tail);
         else
-            launch_dense_lu<T>(b->dense_w, b->G * SW, b->dense_smem, st, B, 2 * P.n_tail);
+            launch_dense_lu<T>(b->dense_w, b->G * SW, b->dense_smem, st, B, 2 * P.n_tail, b->dense_tc);
     }
 }
 
@@ -335,7 +336,7 @@ struct KernelOp {
                     if (b->dense_split)
                         launch_dense_lu_split<T>(G * SW, st, B, 2 * P.n_tail);
                     else
-                        launch_dense_lu<T>(b->dense_w, G * SW, b->dense_smem, st, B, 2 * P.n_tail);
+                        launch_dense_lu<T>(b->dense_w, G * SW, b->dense_smem, st, B, 2 * P.n_tail, b->dense_tc);
                 break;
             case 5: k_solve_fwd<T, SW><<<G, b->threads, 0, st>>>(P, B, B.rhs, 0); break;
             case 6:
@@ -715,11 +716,13 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
         if (cudaGetDevice(&dev) == cudaSuccess)
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
         b->dense_split = b->dense_w == 0 || (L < 2 * (size_t)n_sm && !b->dense_fused);
+        b->dense_tc = opt && opt->dense_tc && !b->dense_split && b->dense_w == 32 &&
+                      b->precision == GAPK_PREC_FP32;
         A(b->Dt, L * N * dense_ld((int)N) * esz);
         if (!b->dense_split) {
             cudaError_t e = b->precision == GAPK_PREC_FP64
-                                ? dense_lu_attributes<double>(b->dense_w, b->dense_smem)
-                                : dense_lu_attributes<float>(b->dense_w, b->dense_smem);
+                                ? dense_lu_attributes<double>(b->dense_w, b->dense_smem, false)
+                                : dense_lu_attributes<float>(b->dense_w, b->dense_smem, b->dense_tc);
             if (e != cudaSuccess) {
                 set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
                 return GAPK_ECUDA;
@@ -1393,7 +1396,7 @@ int noalloc_scratch_ptr(void** out) {
         void* p = nullptr;
         GAPK_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
         for (int w : {32, 16, 8})
-            GAPK_CUDA_TRY(dense_lu_attributes<double>(w, 232448 - 1024));
+            GAPK_CUDA_TRY(dense_lu_attributes<double>(w, 232448 - 1024, false));
         g_noalloc_ptr[dev] = p;
     }
     *out = g_noalloc_ptr[dev];
@@ -1556,7 +1559,7 @@ extern "C" int gapk_nr_solve_noalloc(gapk_nr_plan p, const gapk_nr_inputs* in,
         k_factor<double, 1><<<1, thr, 0, st>>>(P, D);
         if (h.n_tail > 0) {
             k_schur<double, 1><<<blocks_for((long)P.n_schur, 256), 256, 0, st>>>(P, D);
-            launch_dense_lu<double>(dense_w, 1, dense_smem, st, D, (int)N);
+            launch_dense_lu<double>(dense_w, 1, dense_smem, st, D, (int)N, false);
         }
         k_solve_fwd<double, 1><<<1, thr, 0, st>>>(P, D, D.rhs, 0);
         if (h.n_tail > 0)

@@ -895,24 +895,41 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_dense_lu(BatchD
     if (tid == 0 && bad) B.singular[q] = 1;
 }
 
-// Host side: opt in to the kernel's shared memory and launch it for panel width W.
+}  // namespace gapk
+
+#include "dense_lu_tc.cuh"
+
+namespace gapk {
+
+// Host side: opt in to the kernel's shared memory and launch it for panel width W.  With `tc`
+// (FP32, W = 32) the tail is factorised by k_dense_lu_tc instead, the trailing update on the
+// tensor cores; its shared memory does not depend on N.
 template <typename T>
-cudaError_t dense_lu_attributes(int W, size_t smem) {
-    auto set = [&](auto fn) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t dense_lu_attributes(int W, size_t smem, bool tc) {
+    auto set = [&](auto fn, size_t bytes) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         return e;
     };
+    if constexpr (sizeof(T) == 4) {
+        if (tc) return W == 32 ? set(k_dense_lu_tc, dense_lu_tc_smem()) : cudaErrorInvalidValue;
+    }
     switch (W) {
-        case 32: return set(k_dense_lu<T, 32>);
-        case 16: return set(k_dense_lu<T, 16>);
-        case 8: return set(k_dense_lu<T, 8>);
+        case 32: return set(k_dense_lu<T, 32>, smem);
+        case 16: return set(k_dense_lu<T, 16>, smem);
+        case 8: return set(k_dense_lu<T, 8>, smem);
     }
     return cudaErrorInvalidValue;
 }
 
 template <typename T>
-void launch_dense_lu(int W, int grid, size_t smem, cudaStream_t st, BatchDev const& B, int N) {
+void launch_dense_lu(int W, int grid, size_t smem, cudaStream_t st, BatchDev const& B, int N, bool tc) {
+    if constexpr (sizeof(T) == 4) {
+        if (tc) {
+            k_dense_lu_tc<<<grid, 256, dense_lu_tc_smem(), st>>>(B, N);
+            return;
+        }
+    }
     switch (W) {
         case 32: k_dense_lu<T, 32><<<grid, 256, smem, st>>>(B, N); break;
         case 16: k_dense_lu<T, 16><<<grid, 256, smem, st>>>(B, N); break;
