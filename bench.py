@@ -185,7 +185,8 @@ class Clocks:
 # DRAM bytes per scenario per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
 # ncu --set full capture of the kernels on 320 scenarios of the same grid, scaled by scenarios
 # (each scenario's work and bytes are independent of the others).
-MEASURED_TRAFFIC_PER_SCENARIO = {"dense_lu": (1451.877e6 + 1568.291e6) / 320,
+MEASURED_TRAFFIC_PER_SCENARIO = {"dense_lu": (1665.719e6 + 1626.506e6) / 320,  # k_dense_lu_tc
+                                 "dense_lu_fma": (1451.877e6 + 1568.291e6) / 320,  # k_dense_lu
                                  "schur": (103.909e6 + 277.920e6) / 320,
                                  "factor_sparse": (248.066e6 + 205.772e6) / 320}
 
@@ -271,7 +272,7 @@ def run_ours(args, rank, world, device):
     plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
     plan_s = time.perf_counter() - t0
     info = plan.info
-    batch = NRBatch(plan, N_SCEN, use_graph=not args.host_loop, dense_tc=args.dense_tc,
+    batch = NRBatch(plan, N_SCEN, use_graph=not args.host_loop, dense_fma=args.dense_fma,
                     **workloads.batch_kwargs())
     s_dev = torch.as_tensor(s_np, device="cuda")
     v_dev = torch.as_tensor(v_np, device="cuda")
@@ -397,9 +398,10 @@ def run_ours(args, rank, world, device):
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg / (kt[dom] / 1e3) / 1e9
-    tps = MEASURED_TRAFFIC_PER_SCENARIO.get(dom)
+    tps = MEASURED_TRAFFIC_PER_SCENARIO.get(
+        "dense_lu_fma" if dom == "dense_lu" and args.dense_fma else dom)
     traffic = tps * N_SCEN if tps else None
-    # FP32 FMA rate of the dense LU (2/3 N^3 flops per scenario), for the kernels that compute
+    # the dense LU's FP32-accurate flop rate (2/3 N^3 flops per scenario over its time)
     fma_tflops = (N_SCEN * 2.0 / 3.0 * (2 * info["n_tail"]) ** 3 / (kt["dense_lu"] / 1e3) / 1e12
                   if info["n_tail"] and dom == "dense_lu" else None)
     # every kernel of the loop against the same HBM roof (algorithmic bytes / CUDA-event time)
@@ -449,8 +451,8 @@ def run_ours(args, rank, world, device):
             "data": "synthetic (seeded generator, no external dataset)",
             "config": config({"parallelism": f"scenario shards x{world}",
                               "newton_loop": "host" if args.host_loop else "cuda graph",
-                              "dense_lu": "tensor cores (device batch)" if args.dense_tc
-                                          else "cuda-core fma",
+                              "dense_lu_trailing_update": "cuda-core fma (device batch)"
+                                                          if args.dense_fma else "tensor cores",
                               "converged_per_step": conv_all,
                               "max_iterations_run": int(iters.max()), "plan_seconds": plan_s}),
             "e2e": {"value": conv_e2e * args.steps / (e2e_ms / 1e3), "unit": "solves/s",
@@ -462,7 +464,7 @@ def run_ours(args, rank, world, device):
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg,
                          "traffic_source": "ncu capture on 320 scenarios, scaled by scenarios"
                          if traffic else None,
-                         "fp32_fma_tflops": fma_tflops,
+                         "dense_lu_effective_tflops": fma_tflops,
                          "launch_ms": kt[dom], "peak_source": "measured" if peaks else "fallback"},
             "kernel_ms": kt, "kernel_share_ms_per_iter": share, "lu_levels": lu_levels,
             "kernel_roofline": kernel_roofline,
@@ -802,9 +804,9 @@ def main():
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Newton loop from the host instead of one CUDA graph with a "
                          "conditional node (same kernels and work; lets ncu see every launch)")
-    ap.add_argument("--dense-tc", action="store_true",
-                    help="device-resident batch only: the dense-tail LU with its trailing update "
-                         "on the tensor cores (k_dense_lu_tc) instead of CUDA-core FMA")
+    ap.add_argument("--dense-fma", action="store_true",
+                    help="device-resident batch only: the dense-tail LU's trailing update on "
+                         "CUDA-core FMA (k_dense_lu) instead of the tensor cores (k_dense_lu_tc)")
     args = ap.parse_args()
     N_SCEN = args.scenarios
     rank = int(os.environ.get("RANK", "0"))

@@ -62,7 +62,7 @@ class PlanInfo(C.Structure):
 class BatchOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("y_shared", C.c_int), ("lanes", C.c_int),
                 ("threads", C.c_int), ("use_graph", C.c_int), ("dense_fused", C.c_int),
-                ("dense_tc", C.c_int)]
+                ("dense_fma", C.c_int)]
 
 
 class Inputs(C.Structure):

@@ -716,7 +716,7 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
         if (cudaGetDevice(&dev) == cudaSuccess)
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
         b->dense_split = b->dense_w == 0 || (L < 2 * (size_t)n_sm && !b->dense_fused);
-        b->dense_tc = opt && opt->dense_tc && !b->dense_split && b->dense_w == 32 &&
+        b->dense_tc = !(opt && opt->dense_fma) && !b->dense_split && b->dense_w == 32 &&
                       b->precision == GAPK_PREC_FP32;
         A(b->Dt, L * N * dense_ld((int)N) * esz);
         if (!b->dense_split) {

@@ -296,7 +296,7 @@ class NRBatch:
     """Device state for n_scen scenarios sharing one NRPlan."""
 
     def __init__(self, plan: NRPlan, n_scen: int, precision="fp64", y_shared=True, lanes=0,
-                 threads=0, use_graph=True, dense_fused=False, dense_tc=False):
+                 threads=0, use_graph=True, dense_fused=False, dense_fma=False):
         require_cuda()
         self.plan = plan
         self.n_scen = int(n_scen)
@@ -305,7 +305,7 @@ class NRBatch:
         opt = N.BatchOptions(N.PREC_FP64 if precision == "fp64" else N.PREC_FP32,
                              1 if y_shared else 0, int(lanes), int(threads),
                              1 if use_graph else 0, 1 if dense_fused else 0,
-                             1 if dense_tc else 0)
+                             1 if dense_fma else 0)
         h = C.c_void_p()
         N.check(N.lib().gapk_nr_batch_create(plan._h, C.c_int(self.n_scen), C.byref(opt),
                                              C.byref(h)))

@@ -564,10 +564,11 @@ def test_dense_tail_paths_agree():
 
 
 def test_dense_lu_tensor_core_trailing_update():
-    """dense_tc: the one-CTA-per-scenario FP32 dense-tail LU with its rank-32 trailing updates
-    on the tensor cores (tcgen05, three TF32 products per tile accumulated in FP32) converges
-    like the CUDA-core kernel: every scenario converged, iteration counts within one, voltages
-    within 1e-9 of the default kernel's and within 1e-8 of the FP64 oracle."""
+    """The one-CTA-per-scenario FP32 dense-tail LU with its rank-32 trailing updates on the
+    tensor cores (k_dense_lu_tc: tcgen05, three TF32 products per tile accumulated in FP32; the
+    default) converges like the CUDA-core kernel (dense_fma): every scenario converged,
+    iteration counts within one, voltages within 1e-9 of each other and within 1e-8 of the
+    FP64 oracle."""
     torch = _torch()
     from gap_b200 import synth
     from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
@@ -586,20 +587,20 @@ def test_dense_lu_tensor_core_trailing_update():
     v0 = np.repeat(synth.dc_start(net, base)[None], S, axis=0)
     kw = dict(tol=1e-10, max_iter=30, policy="newton", refine=1)
     out = {}
-    for tc in (False, True):
-        r = NRBatch(plan, S, precision="fp32", lanes=8, dense_tc=tc).solve(
+    for fma in (False, True):
+        r = NRBatch(plan, S, precision="fp32", lanes=8, dense_fma=fma).solve(
             y, torch.as_tensor(s_spec, device="cuda"),
             v_init=torch.as_tensor(v0, device="cuda"), **kw)
         torch.cuda.synchronize()
         assert (r.status.cpu().numpy() == 0).all()
-        out[tc] = (r.v.cpu().numpy(), r.iterations.cpu().numpy())
+        out[fma] = (r.v.cpu().numpy(), r.iterations.cpu().numpy())
     assert np.max(np.abs(out[True][0] - out[False][0])) < 1e-9
     assert np.max(np.abs(out[True][1] - out[False][1])) <= 1
     Y = restate.ybus_pi(net)
     for s in (0, 299):
         o = restate.nr_solve(net, Y=Y, tol=1e-12, max_iter=30, base_power=base,
                              policy="newton", jac="exact", s_spec=s_spec[s], v0=v0[s])
-        assert np.max(np.abs(out[True][0][s] - o["v"])) < 1e-8
+        assert np.max(np.abs(out[False][0][s] - o["v"])) < 1e-8
 
 
 def test_host_pipeline_equals_one_batch():
