@@ -253,35 +253,56 @@ __global__ void __launch_bounds__(256, 8) k_mismatch(PlanDev P, BatchDev B) {
     const double2* Yg = B.y_shared ? B.Y : B.Y + (size_t)g * P.nnz_y * SW;
     const int ys = B.y_shared ? 0 : 1;  // Y value of entry p at Yg[p * (ys ? SW : 1) + ys * lane]
     double m = 0.0;
-#pragma unroll 1
-    for (int tile = 0; tile < MM_TILES; ++tile) {
-        const int i = ((blockIdx.x * MM_TILES + tile) * blockDim.x + threadIdx.x) / SW;
-        if (i >= n) break;
-        const int pb = P.y_row_ptr[i], pe = P.y_row_ptr[i + 1];
-        double ir = 0.0, ii = 0.0;
-#pragma unroll 4
-        for (int p = pb; p < pe; ++p) {
-            const double2 y = ys ? Yg[(size_t)p * SW + lane] : Yg[p];
-            const double2 v = Vg[(size_t)P.y_col[p] * SW + lane];
-            ir = fma(y.x, v.x, ir);
-            ir = fma(-y.y, v.y, ir);
-            ii = fma(y.x, v.y, ii);
-            ii = fma(y.y, v.x, ii);
-        }
+    // S = V conj(Y V) and the mismatch of bus i from its accumulated current (vi, sp, t, node:
+    // the bus's own voltage, specified power, type and block node).  Loading these before the
+    // gathers needs more than the 32 registers of 8 CTAs per SM and measured slower.
+    auto finish = [&](int i, double ir, double ii, double2 vi, double2 sp, int t, int node) {
         const size_t o = ((size_t)g * n + i) * SW + lane;
-        const double2 vi = Vg[(size_t)i * SW + lane];
-        // S = V conj(I)
         const double2 s = make_double2(fma(vi.x, ir, vi.y * ii), fma(vi.y, ir, -vi.x * ii));
         B.Scalc[o] = s;
-        const int t = P.bus_type[i];
         if (t != BUS_SLACK) {
-            const double2 sp = B.Sspec[o];
             const double dp = s.x - sp.x;
             const double dq = (t == BUS_PQ) ? s.y - sp.y : 0.0;
-            const int node = P.node_of_bus[i];
             B.rhs[((size_t)g * P.nb + node) * SW + lane] = make_double2(-dp, -dq);
             m = nmax(m, nmax(fabs(dp), fabs(dq)));
         }
+    };
+    // two tiles at a time: the rows of buses i0 and i1 = i0 + 256 / SW are walked together, so
+    // that each thread keeps two independent column -> V gather chains in flight
+#pragma unroll 1
+    for (int tile = 0; tile < MM_TILES; tile += 2) {
+        const int i0 = ((blockIdx.x * MM_TILES + tile) * blockDim.x + threadIdx.x) / SW;
+        const int i1 = i0 + (int)blockDim.x / SW;
+        if (i0 >= n) break;
+        const bool a1 = i1 < n;
+        int p0 = P.y_row_ptr[i0], p1 = a1 ? P.y_row_ptr[i1] : 0;
+        const int e0 = P.y_row_ptr[i0 + 1], e1 = a1 ? P.y_row_ptr[i1 + 1] : 0;
+        double r0 = 0.0, q0 = 0.0, r1 = 0.0, q1 = 0.0;
+        while (p0 < e0 || p1 < e1) {
+            if (p0 < e0) {
+                const double2 y = ys ? Yg[(size_t)p0 * SW + lane] : Yg[p0];
+                const double2 v = Vg[(size_t)P.y_col[p0] * SW + lane];
+                r0 = fma(y.x, v.x, r0);
+                r0 = fma(-y.y, v.y, r0);
+                q0 = fma(y.x, v.y, q0);
+                q0 = fma(y.y, v.x, q0);
+                ++p0;
+            }
+            if (p1 < e1) {
+                const double2 y = ys ? Yg[(size_t)p1 * SW + lane] : Yg[p1];
+                const double2 v = Vg[(size_t)P.y_col[p1] * SW + lane];
+                r1 = fma(y.x, v.x, r1);
+                r1 = fma(-y.y, v.y, r1);
+                q1 = fma(y.x, v.y, q1);
+                q1 = fma(y.y, v.x, q1);
+                ++p1;
+            }
+        }
+        finish(i0, r0, q0, Vg[(size_t)i0 * SW + lane], B.Sspec[((size_t)g * n + i0) * SW + lane],
+               P.bus_type[i0], P.node_of_bus[i0]);
+        if (a1)
+            finish(i1, r1, q1, Vg[(size_t)i1 * SW + lane], B.Sspec[((size_t)g * n + i1) * SW + lane],
+                   P.bus_type[i1], P.node_of_bus[i1]);
     }
 #pragma unroll
     for (int off = SW; off < 32; off <<= 1) m = nmax(m, __shfl_xor_sync(0xffffffffu, m, off));
@@ -1464,6 +1485,13 @@ __global__ void __launch_bounds__(256, 8) k_update(PlanDev P, BatchDev B) {
     const int i = tid / SW, lane = tid % SW;
     if (i >= n) return;
     const int q = g * SW + lane;
+    // the loads that do not depend on the flags below go first (padding lanes have storage),
+    // so that one memory latency covers them and the flags
+    const int node = P.node_of_bus[i];
+    const size_t o = ((size_t)g * n + i) * SW + lane;
+    double2 v = B.V[o];
+    const bool pq = P.bus_type[i] == BUS_PQ;
+    const double2 d = node >= 0 ? B.dx[((size_t)g * P.nb + node) * SW + lane] : make_double2(0.0, 0.0);
     if (q >= B.n_scen) return;  // padding lanes are never updated
     {
         if (B.singular[q]) {
@@ -1478,12 +1506,7 @@ __global__ void __launch_bounds__(256, 8) k_update(PlanDev P, BatchDev B) {
         }
         if (!B.solving[q]) return;
     }
-    const int node = P.node_of_bus[i];
     if (node < 0) return;
-    const double2 d = B.dx[((size_t)g * P.nb + node) * SW + lane];
-    const size_t o = ((size_t)g * n + i) * SW + lane;
-    double2 v = B.V[o];
-    const bool pq = P.bus_type[i] == BUS_PQ;
     if (B.ctrl[3] != 1) {
         // reference policy (cpu_newton_raphson.cpp:457-503): damping 0.9 and the clamps;
         // clamped policy: the same clamps and order with the full step
