@@ -321,6 +321,117 @@ __global__ void __launch_bounds__(256, 2) k_dense_lu_tc(BatchDev B, int N) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(TC_N));
 }
 
+// The split path's trailing update on the tensor cores (FP32): one CTA per (128 x 128 tile of
+// the trailing block, scenario) for the 32-column panel at k0 (its L21 and U12 written by
+// k_dlu_panel), the tile computed as in k_dense_lu_tc -- operands staged hi / lo, 12 MMAs of the
+// transposed product into tensor memory, C loaded while they run, C - D written back from
+// tcgen05.ld registers.  Many CTAs per SM overlap one another's phases.  64 KB of operands, so
+// at most three CTAs share an SM (3 x 128 tensor-memory columns); with k_dense_lu_tc's CTAs on
+// the same SM, shared memory and registers still keep the columns in use below the SM's 512,
+// so the allocation never waits.  The wait on the MMAs is bounded: when it runs out the
+// scenario is marked singular and ctrl[5] set.
+__global__ void __launch_bounds__(256) k_dlu_update_tc(BatchDev B, int N, int k0, int tiles) {
+    constexpr int W = TC_W;
+    const int q = blockIdx.y;
+    if (q >= B.n_scen || !B.solving[q] || (B.gfactor && !B.gfactor[q / B.sw])) return;
+    const int ld = dense_ld(N);
+    float* A = reinterpret_cast<float*>(B.Dt) + (size_t)q * N * ld;
+    const int n2 = N - k0 - W;
+    const int row0 = (blockIdx.x / tiles) * TC_M, col0 = (blockIdx.x % tiles) * TC_N;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    unsigned char* oper = smraw;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tslot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tslot)),
+                     "r"(TC_N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    tc_stage_b(A, ld, k0, n2, col0, oper);
+    tc_stage_a(A, ld, k0, n2, row0, oper);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t taddr = tslot;
+    if (tid == 0) {
+        // F32 accumulate, TF32 A and B, both K-major, N = 128, M = 128
+        constexpr uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
+                                   ((uint32_t)(TC_N >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+        constexpr uint32_t LBO_A = (TC_M / 8) * 128, LBO_B = (TC_N / 8) * 128;
+        const uint32_t base = smem_u32(oper);
+        const uint32_t Ah = base, Al = base + TC_M * W * 4;
+        const uint32_t Bh = base + 2 * TC_M * W * 4, Bl = Bh + TC_N * W * 4;
+        // D^T = U12^T L21^T: tensor-memory lane n holds column n of the update
+        const uint32_t As[3] = {Bh, Bl, Bh}, Bs[3] = {Ah, Ah, Al};
+#pragma unroll
+        for (int pass = 0; pass < 3; ++pass) {
+#pragma unroll
+            for (int j = 0; j < W / 8; ++j) {
+                const uint64_t da = tc_sdesc(As[pass] + 2 * j * LBO_B, LBO_B, 128);
+                const uint64_t db = tc_sdesc(Bs[pass] + 2 * j * LBO_A, LBO_A, 128);
+                const uint32_t accum = (pass | j) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(taddr),
+                    "l"(da), "l"(db), "r"(idesc), "r"(accum));
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mbar))
+                     : "memory");
+    }
+    // this thread's tile column c and rows rb..rb + 63 (its warp's tensor-memory lane quarter
+    // and column half); the first 32 values of C load while the MMAs run
+    const int g = warp & 3, c = g * 32 + lane, rb = (warp >> 2) * 64;
+    const bool cok = col0 + c < n2;
+    float* cbase = A + (size_t)(k0 + W + row0 + rb) * ld + k0 + W + col0 + (cok ? c : 0);
+    const int rows_left = cok ? n2 - row0 - rb : 0;
+    float cv[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+        if (j < rows_left) cv[j] = cbase[j * ld];
+    const bool ok = tc_wait(smem_u32(&mbar), 0u);
+    if (__syncthreads_or(!ok)) {
+        // every thread agrees; wait once more (bounded) for the MMAs before freeing the memory
+        tc_wait(smem_u32(&mbar), 0u);
+        if (tid == 0) {
+            B.singular[q] = 1;
+            B.ctrl[5] = 1;
+        }
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+        for (int half = 0; half < 2; ++half) {
+            float* ch = cbase + (size_t)(32 * half) * ld;
+            const int left = rows_left - 32 * half;
+            if (half == 1) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    if (j < left) cv[j] = ch[j * ld];
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float d[16];
+                tc_ld16(taddr + ((uint32_t)(g * 32) << 16) + (uint32_t)(rb + 32 * half + 16 * h), d);
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (16 * h + j < left) ch[(16 * h + j) * ld] = cv[16 * h + j] - d[j];
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(TC_N));
+}
+
 // Dynamic shared memory of k_dense_lu_tc.
 __host__ __device__ __forceinline__ size_t dense_lu_tc_smem() {
     return (size_t)TC_OPER_BYTES + (2 * TC_W * (TC_W + 4) + TC_W) * 4;

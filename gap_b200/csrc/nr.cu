@@ -159,7 +159,7 @@ struct gapk_nr_batch_s {
     int dense_w = 0;          // panel width of the one-CTA-per-scenario dense LU (0: not used)
     size_t dense_smem = 0;    // its dynamic shared memory
     bool dense_split = false; // factorise the tail with the split kernels
-    bool dense_tc = false;    // the one-CTA-per-scenario LU with the tensor-core trailing update
+    bool dense_tc = false;    // FP32 tail: trailing updates on the tensor cores (either LU path)
     BatchDev dev{};
     // graph cache
     cudaGraph_t graph = nullptr;
@@ -197,7 +197,7 @@ void launch_factor(gapk_nr_batch b, cudaStream_t st) {
         dim3 gs(blocks_for((long)P.n_schur * SW, 256), b->G);
         k_schur<T, SW><<<gs, 256, 0, st>>>(P, B);
         if (b->dense_split)
-            launch_dense_lu_split<T>(b->G * SW, st, B, 2 * P.n_tail);
+            launch_dense_lu_split<T>(b->G * SW, st, B, 2 * P.n_tail, b->dense_tc);
         else
             launch_dense_lu<T>(b->dense_w, b->G * SW, b->dense_smem, st, B, 2 * P.n_tail, b->dense_tc);
     }
@@ -334,7 +334,7 @@ struct KernelOp {
             case 4:
                 if (P.n_tail > 0)
                     if (b->dense_split)
-                        launch_dense_lu_split<T>(G * SW, st, B, 2 * P.n_tail);
+                        launch_dense_lu_split<T>(G * SW, st, B, 2 * P.n_tail, b->dense_tc);
                     else
                         launch_dense_lu<T>(b->dense_w, G * SW, b->dense_smem, st, B, 2 * P.n_tail, b->dense_tc);
                 break;
@@ -716,17 +716,22 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
         if (cudaGetDevice(&dev) == cudaSuccess)
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
         b->dense_split = b->dense_w == 0 || (L < 2 * (size_t)n_sm && !b->dense_fused);
-        b->dense_tc = !(opt && opt->dense_fma) && !b->dense_split && b->dense_w == 32 &&
-                      b->precision == GAPK_PREC_FP32;
+        // FP32 tails have their trailing updates on the tensor cores unless the caller asks for
+        // CUDA-core FMA: k_dense_lu_tc one CTA per scenario (panel width 32), k_dlu_update_tc
+        // on the split path
+        b->dense_tc = !(opt && opt->dense_fma) && b->precision == GAPK_PREC_FP32 &&
+                      (b->dense_split || b->dense_w == 32);
         A(b->Dt, L * N * dense_ld((int)N) * esz);
-        if (!b->dense_split) {
-            cudaError_t e = b->precision == GAPK_PREC_FP64
-                                ? dense_lu_attributes<double>(b->dense_w, b->dense_smem, false)
-                                : dense_lu_attributes<float>(b->dense_w, b->dense_smem, b->dense_tc);
-            if (e != cudaSuccess) {
-                set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-                return GAPK_ECUDA;
-            }
+        cudaError_t e = cudaSuccess;
+        if (!b->dense_split)
+            e = b->precision == GAPK_PREC_FP64
+                    ? dense_lu_attributes<double>(b->dense_w, b->dense_smem, false)
+                    : dense_lu_attributes<float>(b->dense_w, b->dense_smem, b->dense_tc);
+        else if (b->dense_tc)
+            e = split_lu_attributes();
+        if (e != cudaSuccess) {
+            set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+            return GAPK_ECUDA;
         }
     }
     A(b->mis, L * 8);

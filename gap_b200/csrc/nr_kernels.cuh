@@ -1076,16 +1076,29 @@ __global__ void __launch_bounds__(64, sizeof(T) == 4 ? 8 : 4)
 }
 
 // Host side: the split factorisation of every scenario's N x N tail (grid = padded scenarios).
+// With `tc` (FP32) the trailing updates run on the tensor cores (k_dlu_update_tc, 128 x 128
+// tiles; its shared memory opted in by split_lu_attributes).
 template <typename T>
-void launch_dense_lu_split(int grid, cudaStream_t st, BatchDev const& B, int N) {
+void launch_dense_lu_split(int grid, cudaStream_t st, BatchDev const& B, int N, bool tc) {
     for (int k0 = 0; k0 < N; k0 += DLU_W) {
         k_dlu_panel<T><<<grid, 128, 0, st>>>(B, N, k0);
         const int n2 = N - k0 - DLU_W;
         if (n2 > 0) {
+            if constexpr (sizeof(T) == 4) {
+                if (tc) {
+                    const int tt = (n2 + TC_N - 1) / TC_N;
+                    k_dlu_update_tc<<<dim3(tt * tt, grid), 256, TC_OPER_BYTES, st>>>(B, N, k0, tt);
+                    continue;
+                }
+            }
             const int tj = (n2 + DLU_TILE - 1) / DLU_TILE;
             k_dlu_update<T><<<dim3(tj * tj, grid), DLU_TILE, 0, st>>>(B, N, k0, tj);
         }
     }
+}
+inline cudaError_t split_lu_attributes() {
+    return cudaFuncSetAttribute(k_dlu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TC_OPER_BYTES);
 }
 
 // Forward (unit L) then backward (U) substitution on one scenario's tail vector, blocked by

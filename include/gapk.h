@@ -216,10 +216,11 @@ typedef struct {
     int dense_fused;    /* 1: one-CTA-per-scenario dense-tail LU even for a batch too small
                            to fill the GPU alone (batches that run concurrently on several
                            streams); 0: chosen by the batch size                           */
-    int dense_fma;      /* FP32 tails factorised one CTA per scenario have their trailing
-                           update on the tensor cores (k_dense_lu_tc, tcgen05, three TF32
-                           products accumulated in FP32) unless this is 1: then on CUDA-core
-                           FMA (k_dense_lu).  FP64 tails and the split path use CUDA cores.  */
+    int dense_fma;      /* FP32 tails have the trailing updates of their dense LU on the tensor
+                           cores (tcgen05, three TF32 products accumulated in FP32:
+                           k_dense_lu_tc one CTA per scenario, k_dlu_update_tc on the split
+                           path) unless this is 1: then on CUDA-core FMA.  FP64 tails always
+                           use CUDA cores.                                                   */
 } gapk_nr_batch_options;
 
 int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options* opt,

@@ -603,6 +603,45 @@ def test_dense_lu_tensor_core_trailing_update():
         assert np.max(np.abs(out[False][0][s] - o["v"])) < 1e-8
 
 
+def test_split_dense_lu_tensor_core_update():
+    """Batches too small to fill the GPU factorise the dense tail with the split kernels (a
+    panel launch per 32 columns, then one CTA per 128 x 128 trailing tile and scenario); in
+    FP32 the tile update runs on the tensor cores (k_dlu_update_tc).  Against the CUDA-core
+    update (dense_fma): every scenario converged, iterations within one, voltages within 1e-9;
+    against the FP64 oracle within 1e-8."""
+    torch = _torch()
+    from gap_b200 import synth
+    from gap_b200.engine import NRBatch, NRPlan, YbusPlan, branch_params, shunt_params
+
+    net = synth.transmission_grid(3, n=6000)
+    base = 1e8
+    zb = net.u_rated[0] ** 2 / base
+    yp = YbusPlan.from_network(net)
+    y = yp.assemble(torch.as_tensor(branch_params(net), device="cuda"),
+                    torch.as_tensor(shunt_params(net), device="cuda"), mode=1, scale=zb)[0]
+    plan = NRPlan(yp.row_ptr, yp.col_idx, net.bus_type, jacobian="exact")
+    assert 2 * plan.info["n_tail"] > 256 and (2 * plan.info["n_tail"]) % 32
+    S = 8
+    s_spec = synth.load_scenarios(net, S, sigma=0.1, seed=9, base_power=base)
+    v0 = np.repeat(synth.dc_start(net, base)[None], S, axis=0)
+    kw = dict(tol=1e-10, max_iter=30, policy="newton", refine=1)
+    out = {}
+    for fma in (False, True):
+        r = NRBatch(plan, S, precision="fp32", lanes=8, dense_fma=fma).solve(
+            y, torch.as_tensor(s_spec, device="cuda"),
+            v_init=torch.as_tensor(v0, device="cuda"), **kw)
+        torch.cuda.synchronize()
+        assert (r.status.cpu().numpy() == 0).all()
+        out[fma] = (r.v.cpu().numpy(), r.iterations.cpu().numpy())
+    assert np.max(np.abs(out[True][0] - out[False][0])) < 1e-9
+    assert np.max(np.abs(out[True][1] - out[False][1])) <= 1
+    Y = restate.ybus_pi(net)
+    for s in (0, S - 1):
+        o = restate.nr_solve(net, Y=Y, tol=1e-12, max_iter=30, base_power=base,
+                             policy="newton", jac="exact", s_spec=s_spec[s], v0=v0[s])
+        assert np.max(np.abs(out[False][0][s] - o["v"])) < 1e-8
+
+
 def test_host_pipeline_equals_one_batch():
     """Solving from pinned host buffers in two stream-overlapped parts gives bit-identical
     results to one device batch (the parts keep the lane groups)."""
