@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(256, 2) k_dense_lu_tc(BatchDev B, int N) {
 // the same SM, shared memory and registers still keep the columns in use below the SM's 512,
 // so the allocation never waits.  The wait on the MMAs is bounded: when it runs out the
 // scenario is marked singular and ctrl[5] set.
-__global__ void __launch_bounds__(256) k_dlu_update_tc(BatchDev B, int N, int k0, int tiles) {
+__global__ void __launch_bounds__(256, 3) k_dlu_update_tc(BatchDev B, int N, int k0, int tiles) {
     constexpr int W = TC_W;
     const int q = blockIdx.y;
     if (q >= B.n_scen || !B.solving[q] || (B.gfactor && !B.gfactor[q / B.sw])) return;
@@ -388,14 +388,14 @@ __global__ void __launch_bounds__(256) k_dlu_update_tc(BatchDev B, int N, int k0
                      : "memory");
     }
     // this thread's tile column c and rows rb..rb + 63 (its warp's tensor-memory lane quarter
-    // and column half); the first 32 values of C load while the MMAs run
+    // and column half), 16 rows at a time; the first 16 values of C load while the MMAs run
     const int g = warp & 3, c = g * 32 + lane, rb = (warp >> 2) * 64;
     const bool cok = col0 + c < n2;
     float* cbase = A + (size_t)(k0 + W + row0 + rb) * ld + k0 + W + col0 + (cok ? c : 0);
     const int rows_left = cok ? n2 - row0 - rb : 0;
-    float cv[32];
+    float cv[16];
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
+    for (int j = 0; j < 16; ++j)
         if (j < rows_left) cv[j] = cbase[j * ld];
     const bool ok = tc_wait(smem_u32(&mbar), 0u);
     if (__syncthreads_or(!ok)) {
@@ -408,22 +408,19 @@ __global__ void __launch_bounds__(256) k_dlu_update_tc(BatchDev B, int N, int k0
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
-        for (int half = 0; half < 2; ++half) {
-            float* ch = cbase + (size_t)(32 * half) * ld;
-            const int left = rows_left - 32 * half;
-            if (half == 1) {
-#pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    if (j < left) cv[j] = ch[j * ld];
-            }
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                float d[16];
-                tc_ld16(taddr + ((uint32_t)(g * 32) << 16) + (uint32_t)(rb + 32 * half + 16 * h), d);
+        for (int h = 0; h < 4; ++h) {
+            float* ch = cbase + (size_t)(16 * h) * ld;
+            const int left = rows_left - 16 * h;
+            if (h > 0) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j)
-                    if (16 * h + j < left) ch[(16 * h + j) * ld] = cv[16 * h + j] - d[j];
+                    if (j < left) cv[j] = ch[j * ld];
             }
+            float d[16];
+            tc_ld16(taddr + ((uint32_t)(g * 32) << 16) + (uint32_t)(rb + 16 * h), d);
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+                if (j < left) ch[j * ld] = cv[j] - d[j];
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
