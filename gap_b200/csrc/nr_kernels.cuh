@@ -1076,8 +1076,9 @@ __global__ void __launch_bounds__(64, sizeof(T) == 4 ? 8 : 4)
 }
 
 // Host side: the split factorisation of every scenario's N x N tail (grid = padded scenarios).
-// With `tc` (FP32) the trailing updates run on the tensor cores (k_dlu_update_tc, 128 x 128
-// tiles; its shared memory opted in by split_lu_attributes).
+// With `tc` (FP32) the trailing updates of at least one full 128 x 128 tile run on the tensor
+// cores (k_dlu_update_tc; its shared memory opted in by split_lu_attributes); smaller trailing
+// blocks, mostly empty as tensor-core tiles, keep the 64 x 64 CUDA-core tiles.
 template <typename T>
 void launch_dense_lu_split(int grid, cudaStream_t st, BatchDev const& B, int N, bool tc) {
     for (int k0 = 0; k0 < N; k0 += DLU_W) {
@@ -1085,7 +1086,7 @@ void launch_dense_lu_split(int grid, cudaStream_t st, BatchDev const& B, int N, 
         const int n2 = N - k0 - DLU_W;
         if (n2 > 0) {
             if constexpr (sizeof(T) == 4) {
-                if (tc) {
+                if (tc && n2 >= TC_N) {
                     const int tt = (n2 + TC_N - 1) / TC_N;
                     k_dlu_update_tc<<<dim3(tt * tt, grid), 256, TC_OPER_BYTES, st>>>(B, N, k0, tt);
                     continue;
