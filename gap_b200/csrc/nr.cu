@@ -505,7 +505,8 @@ int load_inputs(gapk_nr_batch b, const gapk_nr_inputs* in, cudaStream_t st) {
         return GAPK_EINVAL;
     }
     b->cur_refine = in->refine;
-    int ctrl[5] = {0, in->max_iterations, 1, in->policy, 0};
+    // iteration, max iterations, loop flag, step policy, iterations run, device wait error
+    int ctrl[6] = {0, in->max_iterations, 1, in->policy, 0, 0};
     GAPK_CUDA_TRY(cudaMemcpyAsync(b->ctrl.p, ctrl, sizeof(ctrl), cudaMemcpyHostToDevice, st));
     if (!(in->refine_below >= 0.0) || !(in->reuse_below >= 0.0)) {
         set_error("inputs: refine_below and reuse_below must be >= 0");

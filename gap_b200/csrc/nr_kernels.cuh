@@ -166,6 +166,7 @@ __global__ void k_init_ctrl(BatchDev B, int max_iter, int policy, double tol, do
         B.ctrl[2] = 1;
         B.ctrl[3] = policy;
         B.ctrl[4] = 0;
+        B.ctrl[5] = 0;  // set by a tensor-core LU whose bounded wait ran out during the solve
         B.tol[0] = tol;
         B.tol[1] = refine_below;
         B.tol[2] = reuse_below;
