@@ -38,6 +38,7 @@ EXPORTS = [
     "gapk_nr_stage_get_mismatch", "gapk_nr_stage_kernel", "gapk_nr_solve_noalloc",
     "gapk_nr_step", "gapk_nr_get_state", "gapk_nr_get_outputs", "gapk_nr_level_trace_size",
     "gapk_nr_set_level_trace", "gapk_nr_dense_trace_panels", "gapk_nr_batch_lanes",
+    "gapk_nr_batch_device_error", "gapk_nr_batch_set_wait_test",
     "gapk_splu_create", "gapk_splu_destroy", "gapk_splu_size", "gapk_splu_factorize",
     "gapk_splu_solve", "gapk_nr_adjoint", "gapk_nr_adjoint_branch", "gapk_branch_flows",
 ]

@@ -25,7 +25,7 @@
 // an SM (each holding 128 tensor-memory columns).  Every wait on the mbarrier is bounded: when
 // one runs out (the CTA agrees on it with a barrier), the kernel waits once more, bounded, for
 // the MMAs in flight, marks the scenario singular, sets ctrl[5], frees its tensor memory and
-// ends.
+// ends.  The bound is 200 ms of %globaltimer time (tc_wait).
 #pragma once
 
 #include <cstdint>
@@ -56,17 +56,28 @@ __device__ __forceinline__ void tc_split(float x, float& hi, float& lo) {
     hi = __uint_as_float(u);
     lo = x - hi;
 }
+// Wait for the mbarrier phase `phase` to complete, for at most TC_WAIT_NS of %globaltimer time
+// (and at most 2^24 polls): false when the bound ran out.  A tile's MMAs take about a
+// microsecond; the bound leaves room for the context being time-sliced with others.
+constexpr unsigned long long TC_WAIT_NS = 200000000ull;
 __device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t phase) {
-    uint32_t done = 0;
-    for (int it = 0; it < (1 << 22) && !done; ++it) {
+    unsigned long long t0 = 0;  // read only once a wait lasts (a normal one ends within 64 polls)
+    for (int it = 0; it < (1 << 24); ++it) {
+        uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done)
             : "r"(mbar), "r"(phase)
             : "memory");
+        if (done) return true;
+        if ((it & 63) == 63) {
+            const unsigned long long t = gtimer();
+            if (it == 63) t0 = t;
+            else if (t - t0 > TC_WAIT_NS) return false;
+        }
     }
-    return done != 0;
+    return false;
 }
 // 16 consecutive tensor-memory columns of this thread's lane.
 __device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16]) {
@@ -147,6 +158,7 @@ __global__ void __launch_bounds__(256, 2) k_dense_lu_tc(BatchDev B, int N) {
     if (q >= B.n_scen || !B.solving[q] || (B.gfactor && !B.gfactor[q / B.sw])) return;
     const int ld = dense_ld(N);
     float* A = reinterpret_cast<float*>(B.Dt) + (size_t)q * N * ld;
+    const bool wait_test = B.ctrl[6] != 0;  // test hook: issue no MMAs (the waits run out)
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned char* oper = smraw;
     float* U11 = reinterpret_cast<float*>(smraw + TC_OPER_BYTES);  // [W][W + 4] transposed
@@ -217,7 +229,7 @@ __global__ void __launch_bounds__(256, 2) k_dense_lu_tc(BatchDev B, int N) {
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 __syncthreads();
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                if (tid == 0) {
+                if (tid == 0 && !wait_test) {
                     // the operand address through an opaque move, so that the 24 descriptors
                     // are formed here and not held in registers across the tile loop
                     uint32_t base;
@@ -333,9 +345,13 @@ __global__ void __launch_bounds__(256, 2) k_dense_lu_tc(BatchDev B, int N) {
 __global__ void __launch_bounds__(256, 3) k_dlu_update_tc(BatchDev B, int N, int k0, int tiles) {
     constexpr int W = TC_W;
     const int q = blockIdx.y;
-    if (q >= B.n_scen || !B.solving[q] || (B.gfactor && !B.gfactor[q / B.sw])) return;
+    // a scenario already marked singular (a pivot, or a wait of an earlier panel that ran
+    // out) is not updated further
+    if (q >= B.n_scen || !B.solving[q] || B.singular[q] || (B.gfactor && !B.gfactor[q / B.sw]))
+        return;
     const int ld = dense_ld(N);
     float* A = reinterpret_cast<float*>(B.Dt) + (size_t)q * N * ld;
+    const bool wait_test = B.ctrl[6] != 0;  // test hook: issue no MMAs (the wait runs out)
     const int n2 = N - k0 - W;
     const int row0 = (blockIdx.x / tiles) * TC_M, col0 = (blockIdx.x % tiles) * TC_N;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -360,7 +376,7 @@ __global__ void __launch_bounds__(256, 3) k_dlu_update_tc(BatchDev B, int N, int
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t taddr = tslot;
-    if (tid == 0) {
+    if (tid == 0 && !wait_test) {
         // F32 accumulate, TF32 A and B, both K-major, N = 128, M = 128
         constexpr uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) |
                                    ((uint32_t)(TC_N >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);

@@ -753,6 +753,8 @@ int gapk_nr_batch_create(gapk_nr_plan p, int n_scen, const gapk_nr_batch_options
     // a load (the general LU) refine and refactorise as before
     GAPK_CUDA_TRY(cudaMemset(b->grefine.p, 1, b->grefine.bytes));
     GAPK_CUDA_TRY(cudaMemset(b->gfactor.p, 1, b->gfactor.bytes));
+    // control words: [5] the tensor-core LU's wait error, [6] its wait test (both off)
+    GAPK_CUDA_TRY(cudaMemset(b->ctrl.p, 0, b->ctrl.bytes));
     BatchDev& d = b->dev;
     d.n_scen = n_scen;
     d.n_groups = b->G;
@@ -959,6 +961,26 @@ static int64_t dense_trace_size(gapk_nr_batch b) {
 int64_t gapk_nr_level_trace_size(gapk_nr_batch b) {
     if (!b) return 0;
     return sparse_trace_size(b) + dense_trace_size(b);
+}
+
+int gapk_nr_batch_device_error(gapk_nr_batch b) {
+    if (!b || !b->ctrl.p) return 0;
+    int w = 0;
+    if (cudaMemcpy(&w, b->ctrl.as<int>() + 5, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_error("gapk_nr_batch_device_error: cudaMemcpy failed");
+        return GAPK_ECUDA;
+    }
+    return w ? 1 : 0;
+}
+
+int gapk_nr_batch_set_wait_test(gapk_nr_batch b, int skip) {
+    if (!b || !b->ctrl.p) {
+        set_error("gapk_nr_batch_set_wait_test: null batch");
+        return GAPK_EINVAL;
+    }
+    const int v = skip ? 1 : 0;
+    GAPK_CUDA_TRY(cudaMemcpy(b->ctrl.as<int>() + 6, &v, sizeof(int), cudaMemcpyHostToDevice));
+    return GAPK_OK;
 }
 
 int gapk_nr_dense_trace_panels(gapk_nr_batch b) {

@@ -74,7 +74,8 @@ struct BatchDev {
     double* final_mis;  // [G*SW]
     int* gsolve;      // [G]
     int* giter;       // [G]
-    int* ctrl;        // [0] iteration, [1] max_iter, [2] any iterating, [3] policy, [4] loops
+    int* ctrl;        // [0] iteration, [1] max_iter, [2] any iterating, [3] policy, [4] loops,
+                      // [5] tensor-core LU wait ran out, [6] wait test (skip the MMAs)
     double* tol;      // [0] tolerance, [1] refine below, [2] reuse the factors below this mismatch
                       //     (0: never); the allocation-free path has [0] only
     int* grefine;     // [G] refinement pass runs for the group this iteration (null: always)

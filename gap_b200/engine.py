@@ -315,6 +315,19 @@ class NRBatch:
     def device_bytes(self):
         return int(N.lib().gapk_nr_batch_device_bytes(self._h))
 
+    def device_error(self) -> bool:
+        """True when a bounded wait of the tensor-core dense LU ran out during the last solve
+        (its scenarios end SINGULAR); waits for the device."""
+        rc = int(N.lib().gapk_nr_batch_device_error(self._h))
+        if rc < 0:
+            N.check(rc)
+        return rc == 1
+
+    def set_wait_test(self, skip: bool):
+        """Test hook: with skip the tensor-core dense LU issues no MMAs, so that its bounded
+        waits run out (gapk_nr_batch_set_wait_test)."""
+        N.check(N.lib().gapk_nr_batch_set_wait_test(self._h, C.c_int(1 if skip else 0)))
+
     def _inputs(self, y, s_spec, v_init, u_pu, tol, max_iter, policy, refine, refine_below=0.0,
                 reuse_below=0.0):
         pol = {"reference": N.POLICY_REFERENCE, "newton": N.POLICY_NEWTON,

@@ -317,6 +317,18 @@ int64_t gapk_nr_level_trace_size(gapk_nr_batch b);
 int gapk_nr_dense_trace_panels(gapk_nr_batch b);
 int gapk_nr_set_level_trace(gapk_nr_batch b, unsigned long long* d_stamps, int64_t n_stamps);
 
+/* ==== Bounded waits of the tensor-core dense LU ==========================================
+ * k_dense_lu_tc and k_dlu_update_tc wait for their MMAs on an mbarrier with a bounded number
+ * of polls.  When a wait runs out the CTA marks its scenario SINGULAR, sets the batch's device
+ * error word, frees its tensor memory and returns; the next solve starts with the word clear.
+ * gapk_nr_batch_device_error returns the word (1: a wait ran out during the last solve), after
+ * waiting for the device.  gapk_nr_batch_set_wait_test is a test hook: with skip = 1 the two
+ * kernels issue no MMAs, so that every wait runs out (a factorising scenario then ends
+ * SINGULAR); 0 restores normal operation.  Set it between solves (it is read on the device,
+ * so graphs already built follow it). */
+int gapk_nr_batch_device_error(gapk_nr_batch b);
+int gapk_nr_batch_set_wait_test(gapk_nr_batch b, int skip);
+
 /* ==== Adjoint (gradients through the converged state; no counterpart in the reference) ====
  * With the batch holding a converged state (after gapk_nr_solve, or gapk_nr_stage_load with
  * the solution as d_v_init), refactorises the Jacobian at that state and solves
