@@ -21,8 +21,10 @@
 //     half of its rows, so every load and store of a warp covers 32 adjacent columns of a row;
 //     the first 32 of its 64 C values are loaded while the MMAs run, then C - D is written back
 //     straight from the tcgen05.ld registers, and the next tile's operands are staged.
-// Shared memory is 64 KB of operands plus the panel's L11 / U11 / 1/diag, so three CTAs fit on
-// an SM (each holding 128 tensor-memory columns).  Every wait on the mbarrier is bounded: when
+// Shared memory is 64 KB of operands plus the panel's L11 / U11 / 1/diag and 128 registers per
+// thread, so two CTAs share an SM, holding 128 tensor-memory columns each (with the split
+// path's k_dlu_update_tc beside them, shared memory and registers still keep the columns in use
+// below the SM's 512): the allocation never waits.  Every wait on the mbarrier is bounded: when
 // one runs out (the CTA agrees on it with a barrier), the kernel waits once more, bounded, for
 // the MMAs in flight, marks the scenario singular, sets ctrl[5], frees its tensor memory and
 // ends.  The bound is 200 ms of %globaltimer time (tc_wait).
